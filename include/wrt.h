@@ -1,0 +1,163 @@
+/* wrt.h -- C ABI of the B200 (sm_100a) grid-sampled 3D Radon / ray transform
+ * library (libwrt.so).
+ *
+ * The reference (devhliu/wrt-project) has no library API: its hot path is
+ * four command-line programs whose inner functions are
+ *   plane_integral     radon_grid/src/integral.c:26
+ *   ray_transform      ray_grid/src/integral.c:11
+ *   radon_reduction    radon_reduction/slicing.c:80  (+ ray_interpolate :5)
+ *   radon3d_adjoint    radon_inversion/backprojection/C/src/integral.c:6
+ * each driven by an OpenMP loop nest over the whole output grid.  The entry
+ * points below replace one such program's loop nest each (host buffers in,
+ * host buffers out, same array orders as the programs' text files), plus
+ * device-resident objects for serving.  Every call returns a wrt_status; no
+ * call exits the process.  There is no CPU fallback: without a usable CUDA
+ * device the calls fail with WRT_ERR_NO_DEVICE.
+ *
+ * Array orders (flat, row-major):
+ *   volume  v[ix][iy][iz]          (radon_grid/src/init.c:120-124)
+ *   radon   R[is][iphi][itheta]    (radon_grid/src/radon_grid.c:248-258)
+ *   rays    P[iz][is][iphi]        (ray_grid/src/ray_grid.c:246-255)
+ *   adjoint A[iz][ix][iy]          (backprojection/C/src/radon3d_ajoint.c:240-254)
+ *
+ * Threading: a wrt_ctx is used by one host thread at a time.  A wrt_server
+ * owns its own dispatcher thread; wrt_server_submit/poll may be called from
+ * any thread.
+ */
+#ifndef WRT_H
+#define WRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WRT_ABI_VERSION 1
+
+typedef enum wrt_status {
+  WRT_OK = 0,
+  WRT_ERR_INVALID_ARGUMENT = 1, /* sizes, pointers or options out of range */
+  WRT_ERR_OUT_OF_MEMORY = 2,    /* a device or pinned allocation failed */
+  WRT_ERR_BUDGET = 3,           /* the request does not fit the HBM budget */
+  WRT_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+  WRT_ERR_NO_DEVICE = 5,        /* no usable sm_100 device */
+  WRT_ERR_TIMEOUT = 6,          /* a bounded wait ran out */
+  WRT_ERR_QUEUE_FULL = 7,       /* the server's arrival queue is full */
+  WRT_ERR_NOT_FOUND = 8,        /* unknown request id */
+  WRT_ERR_CANCELLED = 9,        /* the request was cancelled */
+  WRT_ERR_INTERNAL = 10
+} wrt_status;
+
+typedef enum wrt_sampler {
+  WRT_SAMPLER_NEAREST = 0,   /* zero_interp, radon_grid/src/interp.c:63 (reference default) */
+  WRT_SAMPLER_TRILINEAR = 1  /* cube_trilinear_interp, radon_grid/src/interp.c:25 */
+} wrt_sampler;
+
+typedef enum wrt_kernel {
+  WRT_KERNEL_AUTO = 0,   /* staged kernel when it applies */
+  WRT_KERNEL_PLAIN = 1,  /* one warp per plane, gathers through L1 */
+  WRT_KERNEL_STAGED = 2  /* volume layers staged in shared memory, persistent CTAs */
+} wrt_kernel;
+
+/* Options of the plane-integral transform.  Zero-initialised options give the
+ * reference's radon_grid exactly: nearest sampler, lattice [-2n, 2n)^2 with
+ * step 1/n (radon_grid/src/integral.c:38-44). */
+typedef struct wrt_plane_opts {
+  int sampler;     /* wrt_sampler */
+  int half_extent; /* lattice indices i, j in [-L, L); 0 means L = 2n */
+  int kernel;      /* wrt_kernel */
+  int reserved[5];
+} wrt_plane_opts;
+
+typedef struct wrt_ctx wrt_ctx;
+typedef struct wrt_volume wrt_volume;
+typedef struct wrt_grid wrt_grid;
+
+/* ---------------------------------------------------------------- context */
+const char *wrt_status_string(int status);
+int wrt_abi_version(void);
+/* device: CUDA ordinal.  hbm_budget_bytes: cap on the device memory this
+ * context may hold (0 = no cap beyond what the device has). */
+int wrt_ctx_create(int device, size_t hbm_budget_bytes, wrt_ctx **out);
+int wrt_ctx_destroy(wrt_ctx *ctx);
+const char *wrt_ctx_last_error(const wrt_ctx *ctx);
+int wrt_ctx_synchronize(wrt_ctx *ctx);
+/* Bytes of device memory the context currently holds. */
+size_t wrt_ctx_bytes_in_use(const wrt_ctx *ctx);
+/* Number of this library's kernels launched by the context so far. */
+uint64_t wrt_ctx_launch_count(const wrt_ctx *ctx);
+
+/* ------------------------------------------------------------ sphere grid */
+/* n-point Gauss-Legendre nodes (ascending) and weights on [-1,1], computed in
+ * FP64 by Newton's method on the GPU.  Replaces gsl_integration_glfixed_*
+ * (radon_grid/src/init.c:180-187). */
+int wrt_gauss_legendre(wrt_ctx *ctx, int n, double *x, double *w);
+/* The Gauss-uniform Radon grid of radon_grid_init (radon_grid/src/init.c:165)
+ * with the latitude weights of backprojection/C/src/init.c:222-249.
+ * theta_w may be NULL. */
+int wrt_radon_grid_init(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *phi,
+                        double *theta, double *theta_w, double *shift);
+
+/* ------------------------------------------- drop-in transforms, host I/O */
+/* radon_grid: out[is][iphi][itheta] = plane integral over the plane
+ * (shift[is], phi[iphi], theta[itheta]).  Replaces radon_grid.c:229-264 with
+ * plane_integral (radon_grid/src/integral.c:26-58).  opts may be NULL. */
+int wrt_radon_grid(wrt_ctx *ctx, const double *volume, int ngrid, int nphi, int ntheta,
+                   int nshift, const wrt_plane_opts *opts, double *out);
+
+/* ray_grid: out[iz][is][iphi] = ray integral (ray_grid/src/integral.c:11-50,
+ * loop nest ray_grid/src/ray_grid.c:225-262).  frame: NULL for the
+ * reference's z-slices, else a row-major 3x3 rotation applied to every
+ * sample point (layer-by-layer scheme about another axis). */
+int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int ngrid, int nslices, int nshift,
+                 int nphi, const double *frame, double *out);
+
+/* radon_reduction: rays in[iz][is_ray][iphi] (iz < ngrid, the z-slices) to
+ * Radon data out[is][iphi][itheta] (radon_reduction/slicing.c:5-119, loop
+ * nest reduction.c:195-235).  nshift == nshift_ray is the reference; a
+ * different nshift samples the Radon shifts independently of the ray offsets. */
+int wrt_radon_reduction(wrt_ctx *ctx, const double *rays, int ngrid, int nshift_ray,
+                        int nphi, int nshift, int ntheta, double *out);
+
+/* radon3d_grid (backprojection): out[iz][ix][iy] at the cell centres
+ * (radon_inversion/backprojection/C/src/integral.c:6-24 with interp.c:5-28,
+ * loop nest radon3d_ajoint.c:221-260). */
+int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
+                        int nshift, int ngrid, double *out);
+
+/* Exact transpose of wrt_radon_grid with the same options: out_volume (n^3,
+ * v[ix][iy][iz] order) = R^T g.  No counterpart in the reference; it makes
+ * the adjoint identity <R f, g> = <f, R^T g> testable. */
+int wrt_radon_transpose(wrt_ctx *ctx, const double *g, int ngrid, int nphi, int ntheta,
+                        int nshift, const wrt_plane_opts *opts, double *out_volume);
+
+/* ------------------------------------------------ device-resident objects */
+/* A volume held on the device in the layouts the kernels read. */
+int wrt_volume_create(wrt_ctx *ctx, int ngrid, wrt_volume **out);
+/* Upload from host memory (exactly one of f64 / f32 non-NULL), ordered on
+ * the context's stream.  Pinned host memory makes the copy asynchronous. */
+int wrt_volume_upload(wrt_volume *vol, const double *host_f64, const float *host_f32);
+/* Upload from a device buffer of n^3 floats in v[ix][iy][iz] order. */
+int wrt_volume_upload_device(wrt_volume *vol, const float *dev_f32);
+int wrt_volume_destroy(wrt_volume *vol);
+
+/* A sphere grid with its direction tables resident on the device. */
+int wrt_grid_create(wrt_ctx *ctx, int nphi, int ntheta, int nshift, wrt_grid **out);
+int wrt_grid_destroy(wrt_grid *grid);
+
+/* Plane integrals of a resident volume into a device buffer of
+ * nshift*nphi*ntheta doubles (same order as wrt_radon_grid).  Asynchronous on
+ * the context's stream. */
+int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *grid,
+                             const wrt_plane_opts *opts, double *dev_out);
+
+/* The context's CUDA stream (cudaStream_t), for callers that order their own
+ * work against the library's. */
+void *wrt_ctx_stream(wrt_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WRT_H */

@@ -1,0 +1,111 @@
+"""Parity of the CUDA library against the FP64 oracle (small sizes).
+
+Tolerances: the trilinear paths compute in FP32 with compensated sums and must
+stay within relative L2 error 1e-5 of the FP64 oracle; the nearest sampler
+uses the reference's cell choice exactly (guard band re-evaluated in FP64), so
+its only error is FP32 storage of the volume values.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import wrt, rel_l2, rel_max
+
+from wrt_b200.phantom import ellipsoid_phantom, layer_frames
+
+pytestmark = pytest.mark.gpu
+
+TOL_L2 = 1e-5
+
+
+@pytest.fixture(scope="module")
+def vol24():
+    return ellipsoid_phantom(24, 8, 1000)
+
+
+@pytest.fixture(scope="module")
+def volrand():
+    return np.random.default_rng(7).standard_normal((20, 20, 20))
+
+
+def test_gauss_legendre_bit_identical(ctx):
+    for n in (1, 2, 3, 7, 32, 64, 96, 128):
+        x, w = ctx.gauss_legendre(n)
+        xo, wo = O.gauss_legendre(n)
+        assert np.array_equal(x, xo) and np.array_equal(w, wo), n
+
+
+def test_radon_grid_init_matches_oracle(ctx):
+    phi, th, w, s = ctx.radon_grid_init(64, 32, 129)
+    po, to, wo, so = O.radon_grid(64, 32, 129)
+    for a, b in ((phi, po), (th, to), (w, wo), (s, so)):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("sampler", [O.NEAREST, O.TRILINEAR])
+def test_radon_grid_phantom(ctx, vol24, sampler):
+    got = ctx.radon_grid(vol24, 16, 8, 12, sampler=sampler)
+    ref = O.radon_forward(vol24, 16, 8, 12, sampler=sampler)
+    assert rel_l2(got, ref) < TOL_L2
+    assert rel_max(got, ref) < 1e-4
+
+
+@pytest.mark.parametrize("sampler", [O.NEAREST, O.TRILINEAR])
+def test_radon_grid_random_volume(ctx, volrand, sampler):
+    """Non-zero faces: exercises the cube cut-off and the guard band."""
+    got = ctx.radon_grid(volrand, 8, 6, 9, sampler=sampler)
+    ref = O.radon_forward(volrand, 8, 6, 9, sampler=sampler)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+def test_radon_grid_half_extent(ctx, vol24):
+    got = ctx.radon_grid(vol24, 12, 6, 10, sampler=O.TRILINEAR, half_extent=24)
+    ref = O.radon_forward(vol24, 12, 6, 10, sampler=O.TRILINEAR, half_extent=24)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+def test_ray_grid_reference_frame(ctx, vol24, volrand):
+    for v in (vol24, volrand):
+        n = v.shape[0]
+        got = ctx.ray_grid(v, n, 15, 16)
+        ref = O.ray_forward(v, n, 15, 16)
+        assert rel_l2(got, ref) < TOL_L2
+
+
+def test_ray_grid_rotated_frames(ctx, vol24):
+    for F in layer_frames(3, 5)[1:]:
+        got = ctx.ray_grid(vol24, 24, 15, 16, frame=F)
+        ref = O.ray_forward(vol24, 24, 15, 16, frame=F)
+        assert rel_l2(got, ref) < TOL_L2
+
+
+def test_reduction_coupled(ctx, vol24):
+    rays = O.ray_forward(vol24, 24, 20, 16)
+    got = ctx.radon_reduction(rays, 20, 6)
+    ref = O.reduction_forward(rays, 20, 6)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+def test_reduction_decoupled(ctx, vol24):
+    rays = O.ray_forward(vol24, 24, 16, 16)
+    got = ctx.radon_reduction(rays, 31, 8)
+    ref = O.reduction_forward(rays, 31, 8)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+def test_adjoint(ctx):
+    R = np.random.default_rng(3).standard_normal((17, 12, 6))
+    got = ctx.radon3d_adjoint(R, 10)
+    ref = O.adjoint_forward(R, 10)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+@pytest.mark.parametrize("sampler", [O.NEAREST, O.TRILINEAR])
+def test_transpose_inner_product(ctx, vol24, sampler):
+    g = np.random.default_rng(11).standard_normal((10, 12, 6))
+    Rf = ctx.radon_grid(vol24, 12, 6, 10, sampler=sampler)
+    RTg = ctx.radon_transpose(g, 24, sampler=sampler)
+    lhs, rhs = float((Rf * g).sum()), float((vol24 * RTg).sum())
+    assert abs(lhs - rhs) <= 1e-6 * max(abs(lhs), abs(rhs))
+    ref = O.radon_transpose(g, 24, sampler=sampler)
+    assert rel_l2(RTg, ref) < TOL_L2

@@ -1,0 +1,207 @@
+"""Python binding of libwrt (the B200 grid-sampled Radon / ray transform
+library) through its C ABI (include/wrt.h).
+
+The binding mirrors the reference's four programs, one call each:
+
+=====================  ===========================================  ==========
+call                   reference program (loop nest)                 output
+=====================  ===========================================  ==========
+``radon_grid``         radon_grid/src/radon_grid.c:229-264           [s][phi][theta]
+``ray_grid``           ray_grid/src/ray_grid.c:225-262               [z][s][phi]
+``radon_reduction``    radon_reduction/reduction.c:195-235           [s][phi][theta]
+``radon3d_adjoint``    backprojection/C/src/radon3d_ajoint.c:221-260 [z][x][y]
+=====================  ===========================================  ==========
+
+Volumes are ``v[ix][iy][iz]`` arrays, as the reference's text files order
+them.  There is no CPU fallback: every call runs the CUDA library, and a
+missing library or device raises ``WrtError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "lib" / "libwrt.so"
+
+NEAREST, TRILINEAR = 0, 1
+KERNEL_AUTO, KERNEL_PLAIN, KERNEL_STAGED = 0, 1, 2
+
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "out of memory", 3: "over budget", 4: "CUDA error",
+    5: "no device", 6: "timeout", 7: "queue full", 8: "not found", 9: "cancelled", 10: "internal",
+}
+
+
+class WrtError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        super().__init__(f"wrt status {status} ({STATUS.get(status, '?')}): {message}")
+
+
+class PlaneOpts(C.Structure):
+    _fields_ = [("sampler", C.c_int), ("half_extent", C.c_int), ("kernel", C.c_int),
+                ("reserved", C.c_int * 5)]
+
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_vp, _i, _sz = C.c_void_p, C.c_int, C.c_size_t
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libwrt.so (built by ``make -C wrt-project_b200``); raise if absent."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise WrtError(5, f"{LIB_PATH} is missing: build it with `make -C {HERE}`")
+        L = C.CDLL(str(LIB_PATH))
+        L.wrt_status_string.restype = C.c_char_p
+        L.wrt_status_string.argtypes = [_i]
+        L.wrt_abi_version.restype = _i
+        L.wrt_ctx_create.argtypes = [_i, _sz, C.POINTER(_vp)]
+        L.wrt_ctx_destroy.argtypes = [_vp]
+        L.wrt_ctx_last_error.argtypes = [_vp]
+        L.wrt_ctx_last_error.restype = C.c_char_p
+        L.wrt_ctx_synchronize.argtypes = [_vp]
+        L.wrt_ctx_bytes_in_use.argtypes = [_vp]
+        L.wrt_ctx_bytes_in_use.restype = _sz
+        L.wrt_ctx_launch_count.argtypes = [_vp]
+        L.wrt_ctx_launch_count.restype = C.c_uint64
+        L.wrt_ctx_stream.argtypes = [_vp]
+        L.wrt_ctx_stream.restype = _vp
+        L.wrt_gauss_legendre.argtypes = [_vp, _i, _dp, _dp]
+        L.wrt_radon_grid_init.argtypes = [_vp, _i, _i, _i, _dp, _dp, _dp, _dp]
+        L.wrt_radon_grid.argtypes = [_vp, _dp, _i, _i, _i, _i, C.POINTER(PlaneOpts), _dp]
+        L.wrt_ray_grid.argtypes = [_vp, _dp, _i, _i, _i, _i, _vp, _dp]
+        L.wrt_radon_reduction.argtypes = [_vp, _dp, _i, _i, _i, _i, _i, _dp]
+        L.wrt_radon3d_adjoint.argtypes = [_vp, _dp, _i, _i, _i, _i, _dp]
+        L.wrt_radon_transpose.argtypes = [_vp, _dp, _i, _i, _i, _i, C.POINTER(PlaneOpts), _dp]
+        L.wrt_volume_create.argtypes = [_vp, _i, C.POINTER(_vp)]
+        L.wrt_volume_upload.argtypes = [_vp, _vp, _vp]
+        L.wrt_volume_upload_device.argtypes = [_vp, _vp]
+        L.wrt_volume_destroy.argtypes = [_vp]
+        L.wrt_grid_create.argtypes = [_vp, _i, _i, _i, C.POINTER(_vp)]
+        L.wrt_grid_destroy.argtypes = [_vp]
+        L.wrt_radon_forward_device.argtypes = [_vp, _vp, _vp, C.POINTER(PlaneOpts), _vp]
+        _lib = L
+    return _lib
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def plane_opts(sampler=NEAREST, half_extent=0, kernel=KERNEL_AUTO) -> PlaneOpts:
+    o = PlaneOpts()
+    o.sampler, o.half_extent, o.kernel = int(sampler), int(half_extent or 0), int(kernel)
+    return o
+
+
+class Context:
+    """A libwrt context on one CUDA device (its own stream, budget, counters)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0):
+        self._h = _vp()
+        st = lib().wrt_ctx_create(int(device), int(budget_bytes), C.byref(self._h))
+        if st:
+            raise WrtError(st, "wrt_ctx_create")
+
+    # -- plumbing
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().wrt_ctx_destroy(self._h)
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, st: int, what: str):
+        if st:
+            msg = lib().wrt_ctx_last_error(self._h)
+            raise WrtError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    @property
+    def launches(self) -> int:
+        return int(lib().wrt_ctx_launch_count(self._h))
+
+    @property
+    def bytes_in_use(self) -> int:
+        return int(lib().wrt_ctx_bytes_in_use(self._h))
+
+    def synchronize(self):
+        self.check(lib().wrt_ctx_synchronize(self._h), "synchronize")
+
+    # -- grids
+    def gauss_legendre(self, n: int):
+        x, w = np.empty(n), np.empty(n)
+        self.check(lib().wrt_gauss_legendre(self._h, n, x, w), "gauss_legendre")
+        return x, w
+
+    def radon_grid_init(self, nphi: int, ntheta: int, nshift: int):
+        phi, th, w, s = np.empty(nphi), np.empty(ntheta), np.empty(ntheta), np.empty(nshift)
+        self.check(lib().wrt_radon_grid_init(self._h, nphi, ntheta, nshift, phi, th, w, s),
+                   "radon_grid_init")
+        return phi, th, w, s
+
+    # -- drop-in transforms
+    def radon_grid(self, volume, nphi, ntheta, nshift, sampler=NEAREST, half_extent=0,
+                   kernel=KERNEL_AUTO) -> np.ndarray:
+        v = _f64(volume)
+        n = v.shape[0]
+        out = np.empty((nshift, nphi, ntheta))
+        o = plane_opts(sampler, half_extent, kernel)
+        self.check(lib().wrt_radon_grid(self._h, v, n, nphi, ntheta, nshift, C.byref(o), out),
+                   "radon_grid")
+        return out
+
+    def ray_grid(self, volume, nslices, nshift, nphi, frame=None) -> np.ndarray:
+        v = _f64(volume)
+        out = np.empty((nslices, nshift, nphi))
+        f = None if frame is None else _f64(frame).reshape(9)
+        fp = None if f is None else f.ctypes.data_as(_vp)
+        self.check(lib().wrt_ray_grid(self._h, v, v.shape[0], nslices, nshift, nphi, fp, out),
+                   "ray_grid")
+        return out
+
+    def radon_reduction(self, rays, nshift, ntheta) -> np.ndarray:
+        r = _f64(rays)
+        ngrid, nsr, nphi = r.shape
+        out = np.empty((nshift, nphi, ntheta))
+        self.check(lib().wrt_radon_reduction(self._h, r, ngrid, nsr, nphi, nshift, ntheta, out),
+                   "radon_reduction")
+        return out
+
+    def radon3d_adjoint(self, radon, ngrid) -> np.ndarray:
+        R = _f64(radon)
+        nshift, nphi, ntheta = R.shape
+        out = np.empty((ngrid, ngrid, ngrid))
+        self.check(lib().wrt_radon3d_adjoint(self._h, R, nphi, ntheta, nshift, ngrid, out),
+                   "radon3d_adjoint")
+        return out
+
+    def radon_transpose(self, g, ngrid, sampler=TRILINEAR, half_extent=0) -> np.ndarray:
+        g = _f64(g)
+        nshift, nphi, ntheta = g.shape
+        out = np.empty((ngrid, ngrid, ngrid))
+        o = plane_opts(sampler, half_extent)
+        self.check(lib().wrt_radon_transpose(self._h, g, ngrid, nphi, ntheta, nshift, C.byref(o),
+                                             out), "radon_transpose")
+        return out

@@ -1,0 +1,533 @@
+// api.cu -- the C ABI of libwrt (include/wrt.h).
+//
+// Each drop-in entry point replaces one reference program's loop nest:
+//   wrt_radon_grid       radon_grid/src/radon_grid.c:229-264
+//   wrt_ray_grid         ray_grid/src/ray_grid.c:225-262
+//   wrt_radon_reduction  radon_reduction/reduction.c:195-235
+//   wrt_radon3d_adjoint  radon_inversion/backprojection/C/src/radon3d_ajoint.c:221-260
+// Host buffers in, host buffers out; errors come back as wrt_status codes with
+// a message in wrt_ctx_last_error (the reference perror()s and exits).
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+#include <vector>
+
+#include "wrt_internal.cuh"
+
+struct wrt_volume {
+  wrt_ctx *ctx = nullptr;
+  int n = 0;
+  float *d_vol = nullptr;          // n^3, v[ix][iy][iz]
+  unsigned int *d_r2 = nullptr;    // largest |x|^2 of a non-zero node (float bits)
+  float2 *d_pairs = nullptr;       // layer pairs for the staged kernel (lazy)
+  int pitch = 0;
+  size_t vol_bytes = 0, pair_bytes = 0;
+  bool pairs_valid = false;
+};
+
+struct wrt_grid {
+  wrt_ctx *ctx = nullptr;
+  int nphi = 0, ntheta = 0, nshift = 0;
+  std::vector<double> phi, theta, w, shift;
+  double *d_dir = nullptr;    // [nphi*ntheta][9]
+  double *d_shift = nullptr;  // [nshift]
+  size_t bytes = 0;
+};
+
+namespace wrt {
+
+int fail(wrt_ctx *ctx, int status, const char *fmt, ...) {
+  if (ctx) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(ctx->err, sizeof(ctx->err), fmt, ap);
+    va_end(ap);
+  }
+  return status;
+}
+
+int cuda_fail(wrt_ctx *ctx, cudaError_t e, const char *what) {
+  return fail(ctx, WRT_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+int ctx_alloc(wrt_ctx *ctx, void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return WRT_OK;
+  if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+    return fail(ctx, WRT_ERR_BUDGET, "device budget: %zu bytes in use + %zu requested > %zu",
+                ctx->in_use, bytes, ctx->budget);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(ctx, WRT_ERR_OUT_OF_MEMORY, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  ctx->in_use += bytes;
+  return WRT_OK;
+}
+
+void ctx_free(wrt_ctx *ctx, void *p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  ctx->in_use -= bytes;
+}
+
+int check_launch(wrt_ctx *ctx, const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+  return WRT_OK;
+}
+
+}  // namespace wrt
+
+using namespace wrt;
+
+namespace {
+
+// RAII device buffer owned by a context.
+struct DevBuf {
+  wrt_ctx *ctx;
+  void *p = nullptr;
+  size_t bytes = 0;
+  explicit DevBuf(wrt_ctx *c) : ctx(c) {}
+  int alloc(size_t b) {
+    bytes = b;
+    return ctx_alloc(ctx, &p, b);
+  }
+  ~DevBuf() {
+    if (p) ctx_free(ctx, p, bytes);
+  }
+  template <typename T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+int h2d(wrt_ctx *ctx, void *dst, const void *src, size_t bytes, const char *what) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, what);
+}
+
+int d2h_sync(wrt_ctx *ctx, void *dst, const void *src, size_t bytes, const char *what) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, what);
+}
+
+int set_device(wrt_ctx *ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, "cudaSetDevice");
+}
+
+// Reach of a sampler around a lattice point: every node whose value can enter
+// the sample lies within this distance (trilinear: one cell diagonal of the
+// node grid; nearest: cell 2/n plus the offset between cell and node grids).
+double sampler_margin(int n, int sampler) {
+  const double h = 2.0 / (n - 1);
+  const double reach = sampler == WRT_SAMPLER_TRILINEAR ? sqrt(3.0) * h : sqrt(3.0) * (4.0 / n + h);
+  return reach + 1e-6;
+}
+
+bool valid_plane_opts(const wrt_plane_opts *o, int n) {
+  if (!o) return true;
+  if (o->sampler != WRT_SAMPLER_NEAREST && o->sampler != WRT_SAMPLER_TRILINEAR) return false;
+  if (o->half_extent < 0 || o->half_extent > 8 * n) return false;
+  if (o->kernel < WRT_KERNEL_AUTO || o->kernel > WRT_KERNEL_STAGED) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *wrt_status_string(int s) {
+  switch (s) {
+    case WRT_OK: return "ok";
+    case WRT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case WRT_ERR_OUT_OF_MEMORY: return "out of memory";
+    case WRT_ERR_BUDGET: return "over the device-memory budget";
+    case WRT_ERR_CUDA: return "CUDA error";
+    case WRT_ERR_NO_DEVICE: return "no usable CUDA device";
+    case WRT_ERR_TIMEOUT: return "timed out";
+    case WRT_ERR_QUEUE_FULL: return "queue full";
+    case WRT_ERR_NOT_FOUND: return "not found";
+    case WRT_ERR_CANCELLED: return "cancelled";
+    case WRT_ERR_INTERNAL: return "internal error";
+    default: return "unknown status";
+  }
+}
+
+int wrt_abi_version(void) { return WRT_ABI_VERSION; }
+
+int wrt_ctx_create(int device, size_t budget, wrt_ctx **out) {
+  if (!out) return WRT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return WRT_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return WRT_ERR_INVALID_ARGUMENT;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return WRT_ERR_NO_DEVICE;
+  if (prop.major < 10) return WRT_ERR_NO_DEVICE;  // built for sm_100a only
+  wrt_ctx *ctx = new (std::nothrow) wrt_ctx();
+  if (!ctx) return WRT_ERR_OUT_OF_MEMORY;
+  ctx->device = device;
+  ctx->budget = budget;
+  ctx->sm_count = prop.multiProcessorCount;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return WRT_ERR_CUDA;
+  }
+  *out = ctx;
+  return WRT_OK;
+}
+
+int wrt_ctx_destroy(wrt_ctx *ctx) {
+  if (!ctx) return WRT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return WRT_OK;
+}
+
+const char *wrt_ctx_last_error(const wrt_ctx *ctx) { return ctx ? ctx->err : "no context"; }
+
+int wrt_ctx_synchronize(wrt_ctx *ctx) {
+  if (!ctx) return WRT_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, "synchronize");
+}
+
+size_t wrt_ctx_bytes_in_use(const wrt_ctx *ctx) { return ctx ? ctx->in_use : 0; }
+uint64_t wrt_ctx_launch_count(const wrt_ctx *ctx) { return ctx ? ctx->launches : 0; }
+void *wrt_ctx_stream(wrt_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int wrt_gauss_legendre(wrt_ctx *ctx, int n, double *x, double *w) {
+  if (!ctx || !x || !w) return WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  return st ? st : gauss_legendre_device(ctx, n, x, w);
+}
+
+int wrt_radon_grid_init(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *phi,
+                        double *theta, double *theta_w, double *shift) {
+  if (!ctx || !phi || !theta || !shift) return WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  return st ? st : sphere_grid(ctx, nphi, ntheta, nshift, phi, theta, theta_w, shift);
+}
+
+// ------------------------------------------------------------ resident objects
+int wrt_volume_create(wrt_ctx *ctx, int n, wrt_volume **out) {
+  if (!ctx || !out || n < 2 || n > 2048) return WRT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int st = set_device(ctx);
+  if (st) return st;
+  wrt_volume *v = new (std::nothrow) wrt_volume();
+  if (!v) return WRT_ERR_OUT_OF_MEMORY;
+  v->ctx = ctx;
+  v->n = n;
+  v->vol_bytes = sizeof(float) * (size_t)n * n * n;
+  st = ctx_alloc(ctx, (void **)&v->d_vol, v->vol_bytes);
+  if (!st) st = ctx_alloc(ctx, (void **)&v->d_r2, sizeof(unsigned int));
+  if (st) {
+    wrt_volume_destroy(v);
+    return st;
+  }
+  *out = v;
+  return WRT_OK;
+}
+
+int wrt_volume_upload(wrt_volume *v, const double *f64, const float *f32) {
+  if (!v || ((f64 == nullptr) == (f32 == nullptr))) return WRT_ERR_INVALID_ARGUMENT;
+  wrt_ctx *ctx = v->ctx;
+  int st = set_device(ctx);
+  if (st) return st;
+  const size_t count = (size_t)v->n * v->n * v->n;
+  DevBuf stage(ctx);
+  st = stage.alloc(count * (f64 ? sizeof(double) : sizeof(float)));
+  if (!st) st = h2d(ctx, stage.p, f64 ? (const void *)f64 : (const void *)f32, stage.bytes, "volume upload");
+  if (!st)
+    st = f64 ? volume_from_f64(ctx, stage.as<double>(), v->n, v->d_vol, v->d_r2)
+             : volume_from_f32(ctx, stage.as<float>(), v->n, v->d_vol, v->d_r2);
+  if (!st) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);  // the staging buffer dies here
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "volume upload");
+  }
+  v->pairs_valid = false;
+  return st;
+}
+
+int wrt_volume_upload_device(wrt_volume *v, const float *dev_f32) {
+  if (!v || !dev_f32) return WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(v->ctx);
+  if (st) return st;
+  st = volume_from_f32(v->ctx, dev_f32, v->n, v->d_vol, v->d_r2);
+  v->pairs_valid = false;
+  return st;
+}
+
+int wrt_volume_destroy(wrt_volume *v) {
+  if (!v) return WRT_ERR_INVALID_ARGUMENT;
+  wrt_ctx *ctx = v->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx_free(ctx, v->d_vol, v->vol_bytes);
+  ctx_free(ctx, v->d_r2, sizeof(unsigned int));
+  ctx_free(ctx, v->d_pairs, v->pair_bytes);
+  delete v;
+  return WRT_OK;
+}
+
+int wrt_grid_create(wrt_ctx *ctx, int nphi, int ntheta, int nshift, wrt_grid **out) {
+  if (!ctx || !out || nphi < 1 || ntheta < 1 || nshift < 2 || (long long)nphi * ntheta > (1 << 26))
+    return WRT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int st = set_device(ctx);
+  if (st) return st;
+  wrt_grid *g = new (std::nothrow) wrt_grid();
+  if (!g) return WRT_ERR_OUT_OF_MEMORY;
+  g->ctx = ctx;
+  g->nphi = nphi;
+  g->ntheta = ntheta;
+  g->nshift = nshift;
+  g->phi.resize(nphi);
+  g->theta.resize(ntheta);
+  g->w.resize(ntheta);
+  g->shift.resize(nshift);
+  st = sphere_grid(ctx, nphi, ntheta, nshift, g->phi.data(), g->theta.data(), g->w.data(),
+                   g->shift.data());
+  const size_t ndir = (size_t)nphi * ntheta;
+  std::vector<double> dir(ndir * 9);
+  if (!st) {
+    plane_directions(nphi, g->phi.data(), ntheta, g->theta.data(), dir.data());
+    g->bytes = sizeof(double) * (dir.size() + nshift);
+    st = ctx_alloc(ctx, (void **)&g->d_dir, sizeof(double) * dir.size());
+  }
+  if (!st) st = ctx_alloc(ctx, (void **)&g->d_shift, sizeof(double) * nshift);
+  if (!st) st = h2d(ctx, g->d_dir, dir.data(), sizeof(double) * dir.size(), "grid upload");
+  if (!st) st = h2d(ctx, g->d_shift, g->shift.data(), sizeof(double) * nshift, "grid upload");
+  if (!st) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "grid upload");
+  }
+  if (st) {
+    wrt_grid_destroy(g);
+    return st;
+  }
+  *out = g;
+  return WRT_OK;
+}
+
+int wrt_grid_destroy(wrt_grid *g) {
+  if (!g) return WRT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(g->ctx->device);
+  cudaStreamSynchronize(g->ctx->stream);
+  ctx_free(g->ctx, g->d_dir, sizeof(double) * 9 * (size_t)g->nphi * g->ntheta);
+  ctx_free(g->ctx, g->d_shift, sizeof(double) * g->nshift);
+  delete g;
+  return WRT_OK;
+}
+
+int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *grid,
+                             const wrt_plane_opts *opts, double *dev_out) {
+  if (!ctx || !vol || !grid || !dev_out || vol->ctx != ctx || grid->ctx != ctx)
+    return WRT_ERR_INVALID_ARGUMENT;
+  if (!valid_plane_opts(opts, vol->n))
+    return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "invalid plane options");
+  int st = set_device(ctx);
+  if (st) return st;
+  wrt_plane_opts o = {};
+  if (opts) o = *opts;
+  PlaneJob job = {};
+  job.vol = vol->d_vol;
+  job.n = vol->n;
+  job.dir = grid->d_dir;
+  job.shift = grid->d_shift;
+  job.ndir = grid->nphi * grid->ntheta;
+  job.nshift = grid->nshift;
+  job.L = o.half_extent ? o.half_extent : 2 * vol->n;
+  job.sampler = o.sampler;
+  job.r2bits = vol->d_r2;
+  job.margin = sampler_margin(vol->n, o.sampler);
+  job.out = dev_out;
+  return plane_forward_plain(ctx, job);
+}
+
+// -------------------------------------------------------- drop-in, host I/O
+int wrt_radon_grid(wrt_ctx *ctx, const double *volume, int n, int nphi, int ntheta, int nshift,
+                   const wrt_plane_opts *opts, double *out) {
+  if (!ctx || !volume || !out || n < 2 || nphi < 1 || ntheta < 1 || nshift < 2)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon_grid: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
+  if (!valid_plane_opts(opts, n)) return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "invalid plane options");
+  wrt_volume *vol = nullptr;
+  wrt_grid *grid = nullptr;
+  int st = wrt_volume_create(ctx, n, &vol);
+  if (!st) st = wrt_volume_upload(vol, volume, nullptr);
+  if (!st) st = wrt_grid_create(ctx, nphi, ntheta, nshift, &grid);
+  DevBuf dout(ctx);
+  const size_t nout = (size_t)nphi * ntheta * nshift;
+  if (!st) st = dout.alloc(sizeof(double) * nout);
+  if (!st) st = wrt_radon_forward_device(ctx, vol, grid, opts, dout.as<double>());
+  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "radon_grid result");
+  if (grid) wrt_grid_destroy(grid);
+  if (vol) wrt_volume_destroy(vol);
+  return st;
+}
+
+int wrt_radon_transpose(wrt_ctx *ctx, const double *g, int n, int nphi, int ntheta, int nshift,
+                        const wrt_plane_opts *opts, double *out_volume) {
+  if (!ctx || !g || !out_volume || n < 2 || nphi < 1 || ntheta < 1 || nshift < 2)
+    return WRT_ERR_INVALID_ARGUMENT;
+  if (!valid_plane_opts(opts, n)) return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "invalid plane options");
+  wrt_plane_opts o = {};
+  if (opts) o = *opts;
+  wrt_grid *grid = nullptr;
+  int st = wrt_grid_create(ctx, nphi, ntheta, nshift, &grid);
+  DevBuf dg(ctx), dvol(ctx), dvol32(ctx);
+  const size_t nplanes = (size_t)nphi * ntheta * nshift, nvox = (size_t)n * n * n;
+  if (!st) st = dg.alloc(sizeof(double) * nplanes);
+  if (!st) st = dvol.alloc(sizeof(double) * nvox);
+  if (!st) st = h2d(ctx, dg.p, g, sizeof(double) * nplanes, "transpose input");
+  if (!st) {
+    cudaError_t e = cudaMemsetAsync(dvol.p, 0, sizeof(double) * nvox, ctx->stream);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "transpose zero");
+  }
+  if (!st) {
+    PlaneJob job = {};
+    job.n = n;
+    job.dir = grid->d_dir;
+    job.shift = grid->d_shift;
+    job.ndir = nphi * ntheta;
+    job.nshift = nshift;
+    job.L = o.half_extent ? o.half_extent : 2 * n;
+    job.sampler = o.sampler;
+    job.r2bits = nullptr;  // no volume: the whole cube
+    job.margin = 0.0;
+    st = plane_transpose(ctx, job, dg.as<double>(), dvol.as<double>());
+  }
+  if (!st) st = d2h_sync(ctx, out_volume, dvol.p, sizeof(double) * nvox, "transpose result");
+  if (grid) wrt_grid_destroy(grid);
+  return st;
+}
+
+int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int n, int nslices, int nshift, int nphi,
+                 const double *frame, double *out) {
+  if (!ctx || !volume || !out || n < 2 || nslices < 2 || nshift < 2 || nphi < 1)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "ray_grid: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
+  wrt_volume *vol = nullptr;
+  int st = wrt_volume_create(ctx, n, &vol);
+  if (!st) st = wrt_volume_upload(vol, volume, nullptr);
+  // ray_grid/src/init.c:163-176 and the trig of ray_grid/src/integral.c:16-24
+  std::vector<double> shift(nshift), trig(4 * (size_t)nphi);
+  const double dshift = 2.0 / (nshift - 1);
+  for (int i = 0; i < nshift; ++i) shift[i] = (-1.0) + i * dshift;
+  const double dphi = (2 * M_PI) / nphi;
+  for (int i = 0; i < nphi; ++i) {
+    const double phi = dphi * i;
+    trig[4 * i + 0] = cos(phi);
+    trig[4 * i + 1] = sin(phi);
+    trig[4 * i + 2] = cos(phi + M_PI / 2);
+    trig[4 * i + 3] = sin(phi + M_PI / 2);
+  }
+  const bool identity = !frame || (frame[0] == 1.0 && frame[4] == 1.0 && frame[8] == 1.0 &&
+                                   frame[1] == 0.0 && frame[2] == 0.0 && frame[3] == 0.0 &&
+                                   frame[5] == 0.0 && frame[6] == 0.0 && frame[7] == 0.0);
+  DevBuf dshiftb(ctx), dtrig(ctx), dframe(ctx), dout(ctx);
+  const size_t nout = (size_t)nslices * nshift * nphi;
+  if (!st) st = dshiftb.alloc(sizeof(double) * nshift);
+  if (!st) st = dtrig.alloc(sizeof(double) * trig.size());
+  if (!st && !identity) st = dframe.alloc(sizeof(double) * 9);
+  if (!st) st = dout.alloc(sizeof(double) * nout);
+  if (!st) st = h2d(ctx, dshiftb.p, shift.data(), sizeof(double) * nshift, "ray grid");
+  if (!st) st = h2d(ctx, dtrig.p, trig.data(), sizeof(double) * trig.size(), "ray grid");
+  if (!st && !identity) st = h2d(ctx, dframe.p, frame, sizeof(double) * 9, "ray frame");
+  if (!st) {
+    RayJob job = {};
+    job.vol = vol->d_vol;
+    job.n = n;
+    job.nslices = nslices;
+    job.nshift = nshift;
+    job.nphi = nphi;
+    job.trig = dtrig.as<double>();
+    job.shift = dshiftb.as<double>();
+    job.frame = identity ? nullptr : dframe.as<double>();
+    job.r2bits = vol->d_r2;
+    job.margin = sampler_margin(n, WRT_SAMPLER_TRILINEAR);
+    job.out = dout.as<double>();
+    st = ray_forward(ctx, job);
+  }
+  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "ray_grid result");
+  if (vol) wrt_volume_destroy(vol);
+  return st;
+}
+
+int wrt_radon_reduction(wrt_ctx *ctx, const double *rays, int ngrid, int nshift_ray, int nphi,
+                        int nshift, int ntheta, double *out) {
+  if (!ctx || !rays || !out || ngrid < 3 || nshift_ray < 3 || nphi < 1 || nshift < 2 || ntheta < 1)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon_reduction: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  if (st) return st;
+  std::vector<double> phi(nphi), theta(ntheta), w(ntheta), shift(nshift);
+  st = sphere_grid(ctx, nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), shift.data());
+  std::vector<double> cs(2 * (size_t)ntheta);
+  for (int i = 0; i < ntheta; ++i) {
+    cs[2 * i] = cos(theta[i]);  // slicing.c:104-105 evaluate cos/sin(p_theta)
+    cs[2 * i + 1] = sin(theta[i]);
+  }
+  DevBuf drays(ctx), dshift(ctx), dcs(ctx), dout(ctx);
+  const size_t nin = (size_t)ngrid * nshift_ray * nphi, nout = (size_t)nshift * nphi * ntheta;
+  if (!st) st = drays.alloc(sizeof(double) * nin);
+  if (!st) st = dshift.alloc(sizeof(double) * nshift);
+  if (!st) st = dcs.alloc(sizeof(double) * cs.size());
+  if (!st) st = dout.alloc(sizeof(double) * nout);
+  if (!st) st = h2d(ctx, drays.p, rays, sizeof(double) * nin, "reduction input");
+  if (!st) st = h2d(ctx, dshift.p, shift.data(), sizeof(double) * nshift, "reduction grid");
+  if (!st) st = h2d(ctx, dcs.p, cs.data(), sizeof(double) * cs.size(), "reduction grid");
+  if (!st)
+    st = reduction_forward(ctx, drays.as<double>(), ngrid, nshift_ray, nphi, dshift.as<double>(),
+                           nshift, dcs.as<double>(), ntheta, dout.as<double>());
+  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "reduction result");
+  return st;
+}
+
+int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta, int nshift,
+                        int ngrid, double *out) {
+  if (!ctx || !radon || !out || ngrid < 1 || nphi < 1 || ntheta < 1 || nshift < 3)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon3d_adjoint: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  if (st) return st;
+  std::vector<double> phi(nphi), theta(ntheta), w(ntheta), shift(nshift);
+  st = sphere_grid(ctx, nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), shift.data());
+  const int ndir = nphi * ntheta;
+  std::vector<float4> dirw(ndir);
+  const double dphi = 2 * M_PI / nphi;  // backprojection/C/src/integral.c:11
+  for (int ip = 0; ip < nphi; ++ip)
+    for (int it = 0; it < ntheta; ++it)
+      dirw[ip * ntheta + it] = make_float4((float)(sin(theta[it]) * cos(phi[ip])),
+                                           (float)(sin(theta[it]) * sin(phi[ip])),
+                                           (float)cos(theta[it]), (float)(dphi * w[it]));
+  DevBuf dradon(ctx), ddirw(ctx), dout(ctx);
+  const size_t nin = (size_t)nshift * ndir, nout = (size_t)ngrid * ngrid * ngrid;
+  if (!st) st = dradon.alloc(sizeof(double) * nin);
+  if (!st) st = ddirw.alloc(sizeof(float4) * ndir);
+  if (!st) st = dout.alloc(sizeof(double) * nout);
+  if (!st) st = h2d(ctx, dradon.p, radon, sizeof(double) * nin, "adjoint input");
+  if (!st) st = h2d(ctx, ddirw.p, dirw.data(), sizeof(float4) * ndir, "adjoint directions");
+  if (!st)
+    st = adjoint_forward(ctx, dradon.as<double>(), nphi, ntheta, nshift, ddirw.as<float4>(), ngrid,
+                         dout.as<double>());
+  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "adjoint result");
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,242 @@
+// k_spline.cu -- natural cubic splines in the shift variable, the ray-to-Radon
+// reduction (radon_reduction/slicing.c:5-119) and the backprojection adjoint
+// (radon_inversion/backprojection/C/src/integral.c:6-24, interp.c:5-28).
+//
+// The reference builds a GSL natural cubic spline of a whole data line for
+// every single evaluation (slicing.c:45-61, backprojection interp.c:41-45).
+// A line's spline depends only on that line, so here it is built once:
+// spline_prep_kernel solves the natural-spline tridiagonal system of every
+// line (uniform knots s_i = -1 + i h, h = 2/(ns-1), end conditions M_0 =
+// M_{ns-1} = 0) in FP64 and stores, per knot interval, the float4
+// (y_i, y_{i+1}, M_i, M_{i+1}).  An evaluation is then one 16-byte load and
+//   S(s) = a y_i + b y_{i+1} + ((a^3 - a) M_i + (b^3 - b) M_{i+1}) h^2 / 6,
+//   b = (s - s_i)/h, a = 1 - b,
+// the same piecewise cubic as the reference's spline.
+#include <vector>
+
+#include "wrt_internal.cuh"
+
+namespace {
+
+// One thread per line.  src element k of line L is at src[L*line_stride_a +
+// (L / lines_per_group)*... ] -- simplified by the two-level indexing below:
+//   line L = (outer, inner), element e at
+//   src[outer*so + e*se + inner*si].
+// cp[i] / den[i]: forward-elimination coefficients of the (line-independent)
+// tridiagonal matrix, computed on the host.
+__global__ void spline_prep_kernel(const double *__restrict__ src, int nlines, int ninner,
+                                   long long so, long long se, long long si, int ns, double h,
+                                   const double *__restrict__ cp, const double *__restrict__ den,
+                                   double *__restrict__ scratch, float4 *__restrict__ out) {
+  const int L = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L >= nlines) return;
+  const int outer = L / ninner, inner = L % ninner;
+  const double *y = src + outer * so + inner * si;
+  double *M = scratch + (size_t)L * ns;
+  // forward sweep: M holds the modified right-hand sides
+  M[0] = 0.0;
+  M[ns - 1] = 0.0;
+  const double six_h2 = 6.0 / (h * h);
+  double prev = 0.0;
+  for (int i = 1; i + 1 < ns; ++i) {
+    double rhs = six_h2 * (y[(i + 1) * se] - 2.0 * y[i * se] + y[(i - 1) * se]);
+    double dpi = (rhs - (i > 1 ? prev : 0.0)) / den[i];
+    M[i] = dpi;
+    prev = dpi;
+  }
+  for (int i = ns - 3; i >= 1; --i) M[i] = M[i] - cp[i] * M[i + 1];
+  float4 *o = out + (size_t)L * (ns - 1);
+  for (int i = 0; i + 1 < ns; ++i)
+    o[i] = make_float4((float)y[i * se], (float)y[(i + 1) * se], (float)M[i], (float)M[i + 1]);
+}
+
+__device__ __forceinline__ float spline_eval(const float4 *__restrict__ line, int ns, float q,
+                                             float h2_6) {
+  // q = (s + 1)/h in knot units
+  float fi = floorf(q);
+  fi = fminf(fmaxf(fi, 0.0f), (float)(ns - 2));
+  const float b = q - fi, a = 1.0f - b;
+  const float4 c = __ldg(line + (int)fi);
+  return fmaf(a, c.x, b * c.y) + ((a * a - 1.0f) * a * c.z + (b * b - 1.0f) * b * c.w) * h2_6;
+}
+
+// Reduction: one thread per Radon sample (is, iphi, itheta), order of
+// reduction.c:215-229.  Geometry in FP64 with the reference's expressions;
+// spline values and the quadratic in FP32.
+__global__ void __launch_bounds__(256)
+    reduction_kernel(const float4 *__restrict__ lines /* [iz][iphi][ns_ray-1] */, int ngrid,
+                     int ns_ray, int nphi, const double *__restrict__ shift, int nshift,
+                     const double *__restrict__ cs /* [ntheta][2] cos, sin */, int ntheta,
+                     double *__restrict__ out) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)nshift * nphi * ntheta;
+  if (k >= total) return;
+  const int it = (int)(k % ntheta), ip = (int)((k / ntheta) % nphi),
+            is = (int)(k / ((long long)ntheta * nphi));
+  const double p = shift[is], ct = cs[2 * it], st = cs[2 * it + 1];
+  const double dtau = (2.0 / (ngrid - 1)) / (2.0);  // slicing.c:88
+  const double delta_z = 2.0 / (ngrid - 1);         // slicing.c:18
+  const float hs = 2.0f / (float)(ns_ray - 1);
+  const float inv_hs = 1.0f / hs;
+  const float h2_6 = hs * hs / 6.0f;
+  const int half = 2 * ngrid;
+  // |tau| <= sqrt(1 - p^2) bounds the samples that pass slicing.c:110
+  int kmax = half;
+  {
+    double r = 1.0 - p * p;
+    if (r < 0.0) kmax = -1;
+    else kmax = min(half, (int)floor(sqrt(r) / dtau) + 1);
+  }
+  double acc = 0.0;
+  const size_t line_len = (size_t)(ns_ray - 1);
+  for (int itau = -kmax; itau <= kmax; ++itau) {
+    const double tau = __dmul_rn((double)itau, dtau);
+    const double z = __dadd_rn(__dmul_rn(p, ct), __dmul_rn(tau, st));
+    const double s = __dsub_rn(__dmul_rn(p, st), __dmul_rn(tau, ct));
+    if ((fabs(__dadd_rn(__dmul_rn(tau, tau), __dmul_rn(p, p))) > 1.0) || (fabs(z) > 1.0) ||
+        (fabs(s) > 1.0))
+      continue;
+    int iz = (int)__ddiv_rn(__dadd_rn(z, 1.0), delta_z);
+    if (iz == ngrid - 1) iz -= 1;
+    const double z0 = __dadd_rn(-1.0, __dmul_rn(delta_z, (double)iz));
+    const float f = (float)((z - z0) / delta_z);
+    const float q = (float)(s + 1.0) * inv_hs;
+    const float4 *l0 = lines + ((size_t)iz * nphi + ip) * line_len;
+    const float v0 = spline_eval(l0, ns_ray, q, h2_6);
+    const float v1 = spline_eval(l0 + (size_t)nphi * line_len, ns_ray, q, h2_6);
+    const float v2 =
+        iz >= ngrid - 2 ? 0.0f : spline_eval(l0 + 2 * (size_t)nphi * line_len, ns_ray, q, h2_6);
+    // quadratic through (z0, v0), (z0+dz, v1), (z0+2dz, v2) at z0 + f dz
+    const float val = v0 + f * (v1 - v0) + 0.5f * f * (f - 1.0f) * (v2 - 2.0f * v1 + v0);
+    acc += (double)val;
+  }
+  out[k] = acc * dtau;
+}
+
+// Adjoint: one thread per voxel, output order [iz][ix][iy]; loop over all
+// directions.  dirw[d] = (sin t cos p, sin t sin p, cos t, dphi * w_t).
+__global__ void __launch_bounds__(256)
+    adjoint_kernel(const float4 *__restrict__ lines /* [d][ns-1] */, int ndir, int ntheta, int ns,
+                   const float4 *__restrict__ dirw, int n, double *__restrict__ out) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)n * n * n;
+  if (k >= total) return;
+  const int iy = (int)(k % n), ix = (int)((k / n) % n), iz = (int)(k / ((long long)n * n));
+  // cell centres, radon3d_ajoint.c:248-250
+  const float x = (float)((-1.0) + (1.0 / n) + ix * (2.0 / n));
+  const float y = (float)((-1.0) + (1.0 / n) + iy * (2.0 / n));
+  const float z = (float)((-1.0) + (1.0 / n) + iz * (2.0 / n));
+  const float hs = 2.0f / (float)(ns - 1);
+  const float inv_hs = 1.0f / hs;
+  const float h2_6 = hs * hs / 6.0f;
+  const size_t line_len = (size_t)(ns - 1);
+  double acc = 0.0;
+  for (int d0 = 0; d0 < ndir; d0 += ntheta) {
+    float part = 0.0f;
+    const int d1 = min(ndir, d0 + ntheta);
+    for (int d = d0; d < d1; ++d) {
+      const float4 w = __ldg(dirw + d);
+      const float s = fmaf(x, w.x, fmaf(y, w.y, z * w.z));
+      if (fabsf(s) <= 1.0f) part = fmaf(w.w, spline_eval(lines + d * line_len, ns, (s + 1.0f) * inv_hs, h2_6), part);
+    }
+    acc += (double)part;
+  }
+  out[k] = acc;
+}
+
+int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long long so,
+               long long se, long long si, int ns, float4 **d_lines, size_t *bytes) {
+  // line-independent elimination coefficients for the uniform-knot system
+  // h M_{i-1} + 4h M_i + h M_{i+1} = rhs (divided by h: M_{i-1} + 4 M_i + M_{i+1})
+  const double h = 2.0 / (ns - 1);
+  std::vector<double> cp(ns, 0.0), den(ns, 1.0);
+  for (int i = 1; i + 1 < ns; ++i) {
+    den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);
+    cp[i] = 1.0 / den[i];
+  }
+  // the kernel divides rhs by den and uses cp; rhs is 6/h^2 * second difference
+  double *d_coef = nullptr, *d_scratch = nullptr;
+  int st = wrt::ctx_alloc(ctx, (void **)&d_coef, sizeof(double) * 2 * ns);
+  if (st) return st;
+  const size_t scratch_bytes = sizeof(double) * (size_t)nlines * ns;
+  st = wrt::ctx_alloc(ctx, (void **)&d_scratch, scratch_bytes);
+  if (st) {
+    wrt::ctx_free(ctx, d_coef, sizeof(double) * 2 * ns);
+    return st;
+  }
+  *bytes = sizeof(float4) * (size_t)nlines * (ns - 1);
+  st = wrt::ctx_alloc(ctx, (void **)d_lines, *bytes);
+  if (!st) {
+    cudaError_t e = cudaMemcpyAsync(d_coef, cp.data(), sizeof(double) * ns,
+                                    cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_coef + ns, den.data(), sizeof(double) * ns, cudaMemcpyHostToDevice,
+                          ctx->stream);
+    if (e != cudaSuccess) {
+      st = wrt::cuda_fail(ctx, e, "spline coefficients");
+    } else {
+      spline_prep_kernel<<<(nlines + 127) / 128, 128, 0, ctx->stream>>>(
+          d_src, nlines, ninner, so, se, si, ns, h, d_coef, d_coef + ns, d_scratch, *d_lines);
+      ctx->launches++;
+      st = wrt::check_launch(ctx, "spline_prep_kernel");
+      if (!st) {
+        e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = wrt::cuda_fail(ctx, e, "spline prep");
+      }
+    }
+    if (st) wrt::ctx_free(ctx, *d_lines, *bytes);
+  }
+  wrt::ctx_free(ctx, d_scratch, scratch_bytes);
+  wrt::ctx_free(ctx, d_coef, sizeof(double) * 2 * ns);
+  return st;
+}
+
+}  // namespace
+
+namespace wrt {
+
+int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_ray, int nphi,
+                      const double *d_shift, int nshift, const double *d_cs, int ntheta,
+                      double *d_out) {
+  // lines (iz, iphi): element is at d_rays[(iz*ns_ray + is)*nphi + iphi]
+  float4 *d_lines = nullptr;
+  size_t bytes = 0;
+  int st = prep_lines(ctx, d_rays, ngrid * nphi, nphi, (long long)nshift_ray * nphi, nphi, 1,
+                      nshift_ray, &d_lines, &bytes);
+  if (st) return st;
+  const long long total = (long long)nshift * nphi * ntheta;
+  const long long blocks = (total + 255) / 256;
+  reduction_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(d_lines, ngrid, nshift_ray, nphi,
+                                                              d_shift, nshift, d_cs, ntheta, d_out);
+  ctx->launches++;
+  st = check_launch(ctx, "reduction_kernel");
+  if (!st) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "reduction");
+  }
+  ctx_free(ctx, d_lines, bytes);
+  return st;
+}
+
+int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
+                    const float4 *d_dirw, int n, double *d_out) {
+  // lines (iphi, itheta): element is at d_radon[(is*nphi + iphi)*ntheta + itheta]
+  float4 *d_lines = nullptr;
+  size_t bytes = 0;
+  const int ndir = nphi * ntheta;
+  int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, &bytes);
+  if (st) return st;
+  const long long total = (long long)n * n * n;
+  adjoint_kernel<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(
+      d_lines, ndir, ntheta, nshift, d_dirw, n, d_out);
+  ctx->launches++;
+  st = check_launch(ctx, "adjoint_kernel");
+  if (!st) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) st = cuda_fail(ctx, e, "adjoint");
+  }
+  ctx_free(ctx, d_lines, bytes);
+  return st;
+}
+
+}  // namespace wrt

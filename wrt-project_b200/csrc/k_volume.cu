@@ -1,0 +1,89 @@
+// k_volume.cu -- volume preparation.
+//
+// Input: the reference's node-sampled volume v[ix][iy][iz] (radon_grid/src/
+// init.c:120-124), FP64 or FP32.  Output:
+//   * d_vol    FP32 copy in the same order (gathers of the plain kernels and
+//              the guard-band re-evaluation);
+//   * r2bits   the largest squared radius |x|^2 of a non-zero node, as the
+//              bit pattern of a non-negative float (monotone under integer
+//              max).  Every lattice sample farther than sqrt(r2) + sqrt(3)
+//              delta from the origin has only zero corners, so it contributes
+//              exactly 0; the kernels skip those samples.  This is exact for
+//              any input, not an assumption about the support.
+//   * d_pairs  layer pairs for the staged plane kernel: pairs[iz][iy][ix] =
+//              (v[ix][iy][iz], v[ix][iy][iz+1]) for iz in [0, n-2], rows
+//              padded to `pitch` elements so every row starts 16-byte aligned.
+#include "wrt_internal.cuh"
+
+namespace {
+
+template <typename T>
+__global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *__restrict__ dst,
+                                      unsigned int *__restrict__ r2bits) {
+  const size_t total = (size_t)n * n * n;
+  const double h = 2.0 / (n - 1);
+  float local = 0.0f;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    float v = (float)src[k];
+    dst[k] = v;
+    if (v != 0.0f) {
+      int iz = (int)(k % n), iy = (int)((k / n) % n), ix = (int)(k / ((size_t)n * n));
+      double x = -1.0 + h * ix, y = -1.0 + h * iy, z = -1.0 + h * iz;
+      float r2 = (float)(x * x + y * y + z * z) * (1.0f + 1e-6f);
+      local = fmaxf(local, r2);
+    }
+  }
+  // warp max, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) local = fmaxf(local, __shfl_xor_sync(0xffffffffu, local, o));
+  if ((threadIdx.x & 31) == 0 && local > 0.0f) atomicMax(r2bits, __float_as_uint(local));
+}
+
+// pairs[iz][iy][ix] = (v[ix][iy][iz], v[ix][iy][iz+1]); one thread per output.
+__global__ void volume_pairs_kernel(const float *__restrict__ v, int n, float2 *__restrict__ pairs,
+                                    int pitch) {
+  const size_t total = (size_t)(n - 1) * n * pitch;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    int ix = (int)(k % pitch), iy = (int)((k / pitch) % n), iz = (int)(k / ((size_t)pitch * n));
+    float2 p = make_float2(0.0f, 0.0f);
+    if (ix < n) {
+      const float *q = v + ((size_t)ix * n + iy) * n + iz;
+      p = make_float2(q[0], q[1]);
+    }
+    pairs[k] = p;
+  }
+}
+
+template <typename T>
+int convert(wrt_ctx *ctx, const T *d_src, int n, float *d_vol, unsigned int *d_r2bits) {
+  cudaError_t e = cudaMemsetAsync(d_r2bits, 0, sizeof(unsigned int), ctx->stream);
+  if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "volume r2 reset");
+  int blocks = ctx->sm_count * 8;
+  volume_convert_kernel<T><<<blocks, 256, 0, ctx->stream>>>(d_src, n, d_vol, d_r2bits);
+  ctx->launches++;
+  return wrt::check_launch(ctx, "volume_convert_kernel");
+}
+
+}  // namespace
+
+namespace wrt {
+
+int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
+                    unsigned int *d_r2bits) {
+  return convert(ctx, d_src, n, d_vol, d_r2bits);
+}
+
+int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
+                    unsigned int *d_r2bits) {
+  return convert(ctx, d_src, n, d_vol, d_r2bits);
+}
+
+int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch) {
+  int blocks = ctx->sm_count * 8;
+  volume_pairs_kernel<<<blocks, 256, 0, ctx->stream>>>(d_vol, n, d_pairs, pitch);
+  ctx->launches++;
+  return check_launch(ctx, "volume_pairs_kernel");
+}
+
+}  // namespace wrt

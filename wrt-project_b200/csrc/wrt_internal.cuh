@@ -1,0 +1,188 @@
+// wrt_internal.cuh -- shared declarations of libwrt (not part of the ABI).
+//
+// Numerics contract of every volume sampler in this library
+// ---------------------------------------------------------
+// The reference samples in FP64 with two discontinuous rules:
+//   * zero_interp (radon_grid/src/interp.c:63-87): value of the cell
+//     floor((x+1)/(2/n)), clamped to n-1;
+//   * cube_trilinear_interp (radon_grid/src/interp.c:25-60): cell index from
+//     (int)((x+1)/delta) but fraction from fmod(x+1, delta)/delta, which
+//     disagree when x+1 sits within one rounding of a multiple of delta, plus
+//     the upper-boundary clamp, plus the |x| > 1 cut-off.
+// Lattice points produced by the reference's own grids often sit exactly on
+// such boundaries (axis-aligned directions, z-slices on grid nodes), so an
+// FP32 sampler alone would pick different cells there.  Every kernel here
+// therefore computes the cell coordinate q = (x+1)/delta in FP32 and, when
+// frac(q) lies within a guard band g of 0 or 1 (g is several times the
+// worst FP32 error of q), re-evaluates that one sample with the reference's
+// FP64 arithmetic (exact_* below: same operations in the same order, no
+// fused multiply-add).  Outside the band FP32 and FP64 select the same cell
+// and the trilinear value is continuous, so the FP32 result differs from the
+// reference only by rounding.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/wrt.h"
+
+#define WRT_PI 3.14159265358979323846
+
+// ---------------------------------------------------------------- host side
+struct wrt_ctx {
+  int device = 0;
+  size_t budget = 0;      // 0 = unlimited
+  size_t in_use = 0;      // bytes held through ctx_alloc
+  uint64_t launches = 0;  // kernels launched through this context
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  char err[512] = {0};
+};
+
+namespace wrt {
+
+// status helpers (api.cu)
+int fail(wrt_ctx *ctx, int status, const char *fmt, ...);
+int cuda_fail(wrt_ctx *ctx, cudaError_t e, const char *what);
+int ctx_alloc(wrt_ctx *ctx, void **p, size_t bytes);
+void ctx_free(wrt_ctx *ctx, void *p, size_t bytes);
+int check_launch(wrt_ctx *ctx, const char *what);
+
+// Host-side FP64 geometry, computed with the host libm exactly as the
+// reference computes it (radon_grid/src/integral.c:10-36).
+void plane_directions(int nphi, const double *phi, int ntheta, const double *theta,
+                      double *dir9 /* [nphi*ntheta][9]: normal, v1, v2 */);
+// Sphere grid (phi, theta, theta weights, shift) with GL nodes from the GPU.
+int sphere_grid(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *phi,
+                double *theta, double *theta_w, double *shift);
+int gauss_legendre_device(wrt_ctx *ctx, int n, double *x_host, double *w_host);
+
+// Volume preparation kernels (k_volume.cu).
+int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
+                    unsigned int *d_r2bits);
+int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
+                    unsigned int *d_r2bits);
+int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch);
+
+// Plane kernels (k_plane.cu).
+struct PlaneJob {
+  const float *vol;      // n^3 floats, v[ix][iy][iz]
+  const float2 *pairs;   // layer pairs [iz][iy][pitch] (staged kernel) or null
+  int n, pitch;
+  const double *dir;     // [ndir][9] FP64 directions
+  const double *shift;   // [nshift] FP64 shifts
+  int ndir, nshift;
+  int L;                 // lattice half extent
+  int sampler;
+  const unsigned int *r2bits;  // device: largest |x|^2 of a non-zero node (float bits)
+  double margin;         // crop radius = sqrt(r2) + margin (>= the sampler's reach)
+  double *out;           // [nshift][ndir]
+};
+int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job);
+int plane_transpose(wrt_ctx *ctx, const PlaneJob &job, const double *d_g, double *d_vol64);
+
+// Ray kernels (k_ray.cu).
+struct RayJob {
+  const float *vol;
+  int n;
+  int nslices, nshift, nphi;
+  const double *trig;   // [nphi][4]: cos phi, sin phi, cos(phi+pi/2), sin(phi+pi/2)
+  const double *shift;  // [nshift]
+  const double *frame;  // 9 doubles on the device, or null for the z-slices
+  const unsigned int *r2bits;
+  double margin;
+  double *out;          // [nslices][nshift][nphi]
+};
+int ray_forward(wrt_ctx *ctx, const RayJob &job);
+
+// Spline / reduction / adjoint kernels (k_spline.cu).
+int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_ray,
+                      int nphi, const double *d_shift, int nshift,
+                      const double *d_cs /* [ntheta][2]: cos, sin theta */, int ntheta,
+                      double *d_out);
+int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
+                    const float4 *d_dirw /* [nphi*ntheta]: omega, dphi*w */, int n,
+                    double *d_out);
+
+}  // namespace wrt
+
+// ------------------------------------------------------------ device side
+namespace wrtd {
+
+// Reference arithmetic, FP64, no contraction (radon_grid/src/interp.c:3-60).
+__device__ __forceinline__ double lin64(double t, double a, double b) {
+  return __dadd_rn(__dmul_rn(__dsub_rn(1.0, t), a), __dmul_rn(t, b));
+}
+
+__device__ __forceinline__ float ldv(const float *v, int n, int ix, int iy, int iz) {
+  return __ldg(v + ((size_t)ix * n + iy) * n + iz);
+}
+
+// cube_trilinear_interp, radon_grid/src/interp.c:25-60.
+static __device__ __noinline__ double exact_trilinear(const float *v, int n, double x, double y,
+                                               double z) {
+  if ((fabs(x) > 1.0) || (fabs(y) > 1.0) || (fabs(z) > 1.0)) return 0.0;
+  const double delta = __ddiv_rn(2.0, (double)(n - 1));
+  const double x1 = __dadd_rn(x, 1.0), y1 = __dadd_rn(y, 1.0), z1 = __dadd_rn(z, 1.0);
+  int ix = (int)__ddiv_rn(x1, delta), iy = (int)__ddiv_rn(y1, delta),
+      iz = (int)__ddiv_rn(z1, delta);
+  double cx = __ddiv_rn(fmod(x1, delta), delta), cy = __ddiv_rn(fmod(y1, delta), delta),
+         cz = __ddiv_rn(fmod(z1, delta), delta);
+  if (ix == n - 1) { ix -= 1; cx = 1.0; }
+  if (iy == n - 1) { iy -= 1; cy = 1.0; }
+  if (iz == n - 1) { iz -= 1; cz = 1.0; }
+  double a0 = lin64(cx, ldv(v, n, ix, iy, iz), ldv(v, n, ix + 1, iy, iz));
+  double a1 = lin64(cx, ldv(v, n, ix, iy + 1, iz), ldv(v, n, ix + 1, iy + 1, iz));
+  double c0 = lin64(cy, a0, a1);
+  double b0 = lin64(cx, ldv(v, n, ix, iy, iz + 1), ldv(v, n, ix + 1, iy, iz + 1));
+  double b1 = lin64(cx, ldv(v, n, ix, iy + 1, iz + 1), ldv(v, n, ix + 1, iy + 1, iz + 1));
+  double c1 = lin64(cy, b0, b1);
+  return lin64(cz, c0, c1);
+}
+
+// zero_interp, radon_grid/src/interp.c:63-87.
+static __device__ __noinline__ double exact_nearest(const float *v, int n, double x, double y,
+                                             double z) {
+  if ((fabs(x) > 1.0) || (fabs(y) > 1.0) || (fabs(z) > 1.0)) return 0.0;
+  const double delta = __ddiv_rn(2.0, (double)n);
+  int ix = (int)__ddiv_rn(__dadd_rn(x, 1.0), delta), iy = (int)__ddiv_rn(__dadd_rn(y, 1.0), delta),
+      iz = (int)__ddiv_rn(__dadd_rn(z, 1.0), delta);
+  if (ix == n) ix -= 1;
+  if (iy == n) iy -= 1;
+  if (iz == n) iz -= 1;
+  return (double)ldv(v, n, ix, iy, iz);
+}
+
+// FP32 fast path.  q* are cell coordinates ((x+1)/delta for the sampler's
+// delta).  Returns false when the sample must be re-evaluated exactly.
+__device__ __forceinline__ bool in_band(float q, float g) {
+  float f = q - floorf(q);
+  return (f < g) | (f > 1.0f - g);
+}
+
+__device__ __forceinline__ float lerp32(float t, float a, float b) { return fmaf(t, b - a, a); }
+
+// Trilinear from the reference-layout volume at FP32 cell coordinates known
+// to be outside the guard band and inside [0, n-1].
+__device__ __forceinline__ float tri32(const float *__restrict__ v, int n, float qx, float qy,
+                                       float qz) {
+  float fx = floorf(qx), fy = floorf(qy), fz = floorf(qz);
+  float tx = qx - fx, ty = qy - fy, tz = qz - fz;
+  const float *p = v + ((size_t)(int)fx * n + (int)fy) * n + (int)fz;
+  const size_t sx = (size_t)n * n;
+  float c000 = __ldg(p), c001 = __ldg(p + 1), c010 = __ldg(p + n), c011 = __ldg(p + n + 1);
+  float c100 = __ldg(p + sx), c101 = __ldg(p + sx + 1), c110 = __ldg(p + sx + n),
+        c111 = __ldg(p + sx + n + 1);
+  float a0 = lerp32(tx, c000, c100), a1 = lerp32(tx, c010, c110);
+  float b0 = lerp32(tx, c001, c101), b1 = lerp32(tx, c011, c111);
+  float e0 = lerp32(ty, a0, a1), e1 = lerp32(ty, b0, b1);
+  return lerp32(tz, e0, e1);
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+}  // namespace wrtd
