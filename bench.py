@@ -1,0 +1,413 @@
+#!/usr/bin/env python
+"""Benchmark: plane integrals/s of the grid-sampled 3D Radon transform at 128^3.
+
+Workload (one "step"): the forward Radon transform of a 128^3 volume (sum of
+16 seeded ellipsoids, seed 1001) on the Gauss-uniform sphere grid of 64
+latitudes x 128 longitudes x 256 shifts = 2,097,152 plane integrals, each the
+reference's lattice (step 1/n) restricted to [-n, n)^2 = 256 x 256 points with
+the trilinear sampler (radon_grid/src/integral.c:26-58 with
+cube_trilinear_interp).  Synthetic data, generated here.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``value`` is device-timed throughput with the
+volume resident in HBM (CUDA events on the library's stream, L2 flushed before
+every timed step); ``e2e`` is the same metric through the public API with the
+FP64 host volume copied in from pinned memory and the FP64 results copied
+back every step.  ``--impl reference`` times the reference's own C code
+(oracle/_ref, compiled from the reference sources) on the host cores.
+With N > 1 every rank runs the whole workload on its own GPU (independent
+replicas, weak scaling); time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "wrt-project_b200"
+
+N, ELLIPSOIDS, SEED = 128, 16, 1001
+NPHI, NTHETA, NSHIFT = 128, 64, 256
+HALF_EXTENT = N  # lattice [-n, n)^2 -> 256 x 256 samples per plane
+BYTES_PER_SAMPLE = 32  # eight FP32 voxel reads per trilinear sample
+METRIC = "plane integrals/s @128^3 (64x128 sphere grid x 256 shifts, trilinear, 256^2 lattice)"
+UNIT = "plane integrals/s"
+
+
+def load_package():
+    spec = importlib.util.spec_from_file_location(
+        "wrt_b200", PKG_DIR / "__init__.py", submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["wrt_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ------------------------------------------------------------ distributed
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.lines = device, None, []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU baselines
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def plane_sample(count: int, seed: int):
+    """A seeded random subset of the workload's planes (phi, theta, shift)."""
+    sys.path.insert(0, str(ROOT))
+    import oracle as O
+
+    phi, theta, _, shift = O.radon_grid(NPHI, NTHETA, NSHIFT)
+    rng = np.random.default_rng(seed)
+    idx = rng.integers(0, NPHI * NTHETA * NSHIFT, size=count)
+    it, ip, i_s = idx % NTHETA, (idx // NTHETA) % NPHI, idx // (NTHETA * NPHI)
+    return phi[ip], theta[it], shift[i_s]
+
+
+def time_reference_planes(vol, count, seed, threads):
+    """The reference's plane_integral (nearest sampler, lattice [-2n,2n)^2, as
+    shipped in radon_grid) over `count` sampled planes; returns planes/s."""
+    sys.path.insert(0, str(ROOT))
+    import oracle as O
+
+    ref = O.Reference()
+    p, t, s = plane_sample(count, seed)
+    t0 = time.perf_counter()
+    ref.plane_integrals(vol, p, t, s, nthreads=threads)
+    return count / (time.perf_counter() - t0)
+
+
+def cpu_baseline(vol, budget_s=12.0):
+    threads = cpu_threads()
+    sys.path.insert(0, str(ROOT))
+    import oracle as O
+
+    if not O.Reference.available():
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": "oracle/_ref not built"}
+    # calibrate on a small sample, then size the measured sample to ~budget_s
+    rate = time_reference_planes(vol, 256, 1, threads)
+    count = int(max(512, min(200000, rate * budget_s)))
+    rate = time_reference_planes(vol, count, 2, threads)
+    # the FP64 restatement with the benchmark's own sampler and lattice
+    p, t, s = plane_sample(max(256, count // 8), 3)
+    t0 = time.perf_counter()
+    O.radon_planes(vol, p, t, s, sampler=O.TRILINEAR, half_extent=HALF_EXTENT, nthreads=threads)
+    port_rate = len(p) / (time.perf_counter() - t0)
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{count} seeded random planes of the 128^3 workload; the reference's "
+                      f"radon_grid plane_integral as shipped (nearest sampler, 512^2 lattice, "
+                      f"FP64), gcc -O2, OpenMP over planes",
+            "port_trilinear": {"value": port_rate, "unit": UNIT, "kind": "port",
+                               "sample": f"{len(p)} planes, the benchmark's own definition "
+                                         f"(trilinear, 256^2 lattice), FP64 oracle restatement"}}
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return 0
+    sys.path.insert(0, str(PKG_DIR))
+    from phantom import ellipsoid_phantom
+    sys.path.insert(0, str(ROOT))
+    import oracle as O
+
+    threads = cpu_threads()
+    if not O.Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built "
+                          "(reference sources were not present at build time)"}))
+        return 0
+    vol = ellipsoid_phantom(N, ELLIPSOIDS, SEED)
+    per_step = int(os.environ.get("WRT_REF_PLANES_PER_STEP", "2048"))
+    for w in range(args.warmup):
+        time_reference_planes(vol, per_step, 100 + w, threads)
+    t_total = 0.0
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        time_reference_planes(vol, per_step, 1000 + k, threads)
+        t_total += time.perf_counter() - t0
+    value = per_step * args.steps / t_total
+    ms_per_step = 1e3 * t_total / args.steps
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "radon_grid 128^3, 64x128x256 planes", "n": N,
+                   "sphere_grid": [NTHETA, NPHI], "shifts": NSHIFT,
+                   "per_step": f"{per_step} seeded random planes of the workload"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{per_step} planes per step; radon_grid plane_integral as "
+                                   f"shipped (nearest sampler, 512^2 lattice), FP64"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------ our arm
+def traffic_from_profiles():
+    """DRAM bytes per launch of the plane kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "plane_kernel_128cubed.md"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args, dist):
+    wrt = load_package()
+    from wrt_b200.phantom import ellipsoid_phantom
+
+    dev = dist.local_rank
+    ctx = wrt.Context(dev)
+    phantom = ellipsoid_phantom(N, ELLIPSOIDS, SEED)
+    vol = wrt.Volume(ctx, N)
+    vol.upload(phantom)
+    grid = wrt.Grid(ctx, NPHI, NTHETA, NSHIFT)
+    nplanes = grid.nplanes
+    out = wrt.DeviceBuffer(ctx, nplanes * 8)
+    kernel = {"plain": wrt.KERNEL_PLAIN, "staged": wrt.KERNEL_STAGED, "auto": wrt.KERNEL_AUTO}[args.kernel]
+
+    def step(k=kernel):
+        wrt.radon_forward_device(ctx, vol, grid, out.ptr, sampler=wrt.TRILINEAR,
+                                 half_extent=HALF_EXTENT, kernel=k)
+
+    # samples evaluated per launch (one counted launch, outside the timed region)
+    ctx.count_samples(True)
+    step()
+    samples = ctx.sample_count()
+    ctx.count_samples(False)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ctx.synchronize()
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    dist.barrier()
+    ctx.synchronize()
+    launches0 = ctx.launches
+    times = []
+    for _ in range(args.steps):
+        ctx.flush_l2()
+        ctx.timer_start()
+        step()
+        times.append(ctx.timer_stop())
+    launches = ctx.launches - launches0
+    ctx.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    total_ms = dist.max(sum(times))
+    ms_per_step = total_ms / args.steps
+    value = nplanes * args.steps * dist.world / (total_ms * 1e-3)
+
+    # plain kernel alongside (the one-request-per-launch baseline)
+    plain = None
+    if kernel != wrt.KERNEL_PLAIN:
+        step(wrt.KERNEL_PLAIN)
+        pt = []
+        for _ in range(max(2, min(args.steps, 5))):
+            ctx.flush_l2()
+            ctx.timer_start()
+            step(wrt.KERNEL_PLAIN)
+            pt.append(ctx.timer_stop())
+        plain = {"value": nplanes / (statistics.mean(pt) * 1e-3), "unit": UNIT,
+                 "ms_per_step": statistics.mean(pt)}
+
+    # end to end through the public API: FP64 volume in from pinned host
+    # memory, resident grid, FP64 results back to pinned host memory
+    pin_in = wrt.PinnedArray(ctx, (N, N, N), np.float64)
+    pin_in.array[...] = phantom
+    pin_out = wrt.PinnedArray(ctx, (NSHIFT, NPHI, NTHETA), np.float64)
+    for _ in range(2):
+        vol.upload(pin_in.array)
+        step()
+        out.download(pin_out.array)
+    dist.barrier()
+    e2e_times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        vol.upload(pin_in.array)
+        step()
+        out.download(pin_out.array)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_total = dist.max(sum(e2e_times))
+    e2e_value = nplanes * args.steps * dist.world / e2e_total
+
+    # roofline of the plane kernel: 32 B of staged voxel reads per sample
+    # against the measured shared-memory bandwidth of this device
+    smem_bw = ctx.smem_bandwidth()
+    per_launch_s = ms_per_step * 1e-3
+    achieved = samples * BYTES_PER_SAMPLE / per_launch_s / 1e9
+    peak = smem_bw / 1e9
+    hbm_bytes = N ** 3 * 4 + nplanes * 8  # compulsory: FP32 volume in, FP64 results out
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    hbm_peak = json.loads(peaks_file.read_text()).get("hbm_gbs") if peaks_file.exists() else 6650.0
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "radon_grid forward, 128^3 volume of 16 seeded ellipsoids, "
+                               "64x128 Gauss-uniform sphere grid x 256 shifts, trilinear, "
+                               "lattice step 1/n on [-n,n)^2",
+                   "n": N, "sphere_grid": [NTHETA, NPHI], "shifts": NSHIFT,
+                   "planes_per_step": nplanes, "kernel": args.kernel,
+                   "l2": "flushed before every timed step (2x L2 memset)",
+                   "parallelism": f"replicas x{dist.world}"},
+        "samples_per_step": samples,
+        "samples_per_s": samples * args.steps * dist.world / (total_ms * 1e-3),
+        "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
+        "gpu_launches": launches,
+        "roofline": {"bound": "l1tex", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic_from_profiles(),
+                     "peak_source": "shared-memory read bandwidth measured in this run "
+                                    "(wrt_measure_smem_bandwidth); 32 B per trilinear sample",
+                     "hbm": {"achieved": hbm_bytes / per_launch_s / 1e9, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": hbm_bytes / per_launch_s / 1e9 / hbm_peak,
+                             "note": "compulsory bytes only; the volume is re-read from L2"}},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N ** 3 * 8,
+                "d2h_bytes_per_step": nplanes * 8},
+        "clocks": clk,
+    }
+    if plain:
+        result["plain"] = plain
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(phantom)
+    if dist.rank == 0:
+        print(json.dumps(result))
+    pin_in.close()
+    pin_out.close()
+    out.close()
+    vol.close()
+    grid.close()
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--kernel", choices=["auto", "plain", "staged"], default="auto")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default=None,
+                    help="NPHI,NTHETA,NSHIFT: a smaller sphere grid (profiling captures only)")
+    args = ap.parse_args()
+    if args.grid:
+        global NPHI, NTHETA, NSHIFT
+        NPHI, NTHETA, NSHIFT = (int(x) for x in args.grid.split(","))
+    dist = Dist(args.gpus)
+    try:
+        rc = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+    finally:
+        dist.close()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

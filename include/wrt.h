@@ -157,6 +157,33 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid
  * work against the library's. */
 void *wrt_ctx_stream(wrt_ctx *ctx);
 
+/* Caller-owned device and pinned host memory, counted against the context's
+ * budget (device) and released with the matching free. */
+int wrt_device_alloc(wrt_ctx *ctx, size_t bytes, void **dev_ptr);
+int wrt_device_free(wrt_ctx *ctx, void *dev_ptr);
+int wrt_host_alloc_pinned(wrt_ctx *ctx, size_t bytes, void **host_ptr);
+int wrt_host_free_pinned(wrt_ctx *ctx, void *host_ptr);
+/* Copies ordered on the context's stream; the device-to-host copy waits. */
+int wrt_copy_to_device(wrt_ctx *ctx, void *dev_dst, const void *host_src, size_t bytes);
+int wrt_copy_to_host(wrt_ctx *ctx, void *host_dst, const void *dev_src, size_t bytes);
+
+/* ------------------------------------------------------------ measurement */
+/* CUDA-event timer on the context's stream: start records an event, stop
+ * records a second one, waits for it and returns the elapsed milliseconds. */
+int wrt_ctx_timer_start(wrt_ctx *ctx);
+int wrt_ctx_timer_stop(wrt_ctx *ctx, float *ms);
+/* Overwrite a device buffer larger than the L2 cache (evicts the volume). */
+int wrt_ctx_flush_l2(wrt_ctx *ctx);
+/* When on, the plane kernels count the lattice samples they evaluate (one
+ * atomic per plane).  wrt_ctx_sample_count waits for the stream and returns
+ * the running total. */
+int wrt_ctx_count_samples(wrt_ctx *ctx, int on);
+int wrt_ctx_sample_count(wrt_ctx *ctx, uint64_t *count);
+/* Shared-memory read bandwidth of the whole device (bytes/s), measured by a
+ * conflict-free 16-byte-per-lane load loop on every SM: the ceiling of the
+ * gather kernels, whose samples read 32 bytes of staged volume each. */
+int wrt_measure_smem_bandwidth(wrt_ctx *ctx, double *bytes_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,8 +76,14 @@ double gsl_interp_eval(const gsl_interp *p, const double xa[], const double ya[]
                        double x, gsl_interp_accel *a) {
   (void)a;
   if (x < p->xmin || x > p->xmax) {
-    fprintf(stderr, "gsl_shim: interpolation error (x=%.17g outside [%.17g, %.17g])\n",
-            x, p->xmin, p->xmax);
+    /* GSL's default error handler aborts the program here; the shim reports
+     * the first occurrence and returns NaN (GSL with the handler off). */
+    static int reported = 0;
+    if (!reported) {
+      reported = 1;
+      fprintf(stderr, "gsl_shim: interpolation error (x=%.17g outside [%.17g, %.17g]); "
+              "GSL would abort here, the shim returns NaN\n", x, p->xmin, p->xmax);
+    }
     return NAN;
   }
   if (p->type->kind == 1) return orc_spline_eval(xa, ya, p->work, p->size, x);

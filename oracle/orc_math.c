@@ -2,11 +2,30 @@
 #include "orc_math.h"
 #include <math.h>
 
+/* The Gauss-Legendre generator uses only IEEE basic operations (+ - * /,
+ * fabs) in a fixed order, so that the same algorithm compiled for the GPU
+ * (wrt-project_b200/csrc/k_grid.cu, built without fused multiply-add)
+ * produces bit-identical nodes and weights.  The initial guess therefore uses
+ * a Maclaurin series for the cosine instead of libm. */
+static double series_cos(double a) { /* a in [0, pi] */
+  double a2 = a * a, term = 1.0, sum = 1.0;
+  for (int k = 1; k <= 30; ++k) {
+    double den = (double)((2 * k - 1) * (2 * k));
+    term = ((-term) * a2) / den;
+    sum = sum + term;
+  }
+  return sum;
+}
+
 static void legendre_pair(int n, double x, double *pn, double *pnm1) {
   double p0 = 1.0, p1 = x;
   if (n == 0) { *pn = 1.0; *pnm1 = 0.0; return; }
   for (int k = 1; k < n; ++k) {
-    double p2 = ((2.0 * k + 1.0) * x * p1 - k * p0) / (k + 1.0);
+    double kd = (double)k;
+    double a = 2.0 * kd + 1.0;
+    double t = (a * x) * p1;
+    double num = t - kd * p0;
+    double p2 = num / (kd + 1.0);
     p0 = p1;
     p1 = p2;
   }
@@ -14,23 +33,29 @@ static void legendre_pair(int n, double x, double *pn, double *pnm1) {
   *pnm1 = p0;
 }
 
+static double legendre_deriv(int n, double r, double pn, double pnm1) {
+  double num = (double)n * (r * pn - pnm1);
+  double den = r * r - 1.0;
+  return num / den;
+}
+
 int orc_gl_nodes(int n, double *x, double *w) {
   if (n < 1) return -1;
   const int m = n / 2; /* number of strictly positive roots */
   for (int k = 1; k <= m; ++k) {
-    /* Tricomi-style initial guess for the k-th largest root. */
-    double r = cos(M_PI * (k - 0.25) / (n + 0.5));
+    double ang = (M_PI * ((double)k - 0.25)) / ((double)n + 0.5);
+    double r = series_cos(ang); /* k-th largest root, initial guess */
     double pn, pnm1, dp;
     for (int it = 0; it < 100; ++it) {
       legendre_pair(n, r, &pn, &pnm1);
-      dp = n * (r * pn - pnm1) / (r * r - 1.0);
+      dp = legendre_deriv(n, r, pn, pnm1);
       double dr = pn / dp;
-      r -= dr;
+      r = r - dr;
       if (fabs(dr) <= 1e-16 * fabs(r)) break;
     }
     legendre_pair(n, r, &pn, &pnm1);
-    dp = n * (r * pn - pnm1) / (r * r - 1.0);
-    double wk = 2.0 / ((1.0 - r * r) * dp * dp);
+    dp = legendre_deriv(n, r, pn, pnm1);
+    double wk = 2.0 / (((1.0 - r * r) * dp) * dp);
     /* ascending order: negative roots first, mirrored exactly */
     x[k - 1] = -r;
     w[k - 1] = wk;
@@ -40,9 +65,9 @@ int orc_gl_nodes(int n, double *x, double *w) {
   if (n & 1) {
     double pn, pnm1;
     legendre_pair(n, 0.0, &pn, &pnm1);
-    double dp = n * (0.0 * pn - pnm1) / (0.0 - 1.0);
+    double dp = legendre_deriv(n, 0.0, pn, pnm1);
     x[m] = 0.0;
-    w[m] = 2.0 / (dp * dp);
+    w[m] = 2.0 / ((1.0 * dp) * dp);
   }
   return 0;
 }

@@ -88,6 +88,18 @@ def lib() -> C.CDLL:
         L.wrt_grid_create.argtypes = [_vp, _i, _i, _i, C.POINTER(_vp)]
         L.wrt_grid_destroy.argtypes = [_vp]
         L.wrt_radon_forward_device.argtypes = [_vp, _vp, _vp, C.POINTER(PlaneOpts), _vp]
+        L.wrt_ctx_timer_start.argtypes = [_vp]
+        L.wrt_ctx_timer_stop.argtypes = [_vp, C.POINTER(C.c_float)]
+        L.wrt_ctx_flush_l2.argtypes = [_vp]
+        L.wrt_ctx_count_samples.argtypes = [_vp, _i]
+        L.wrt_ctx_sample_count.argtypes = [_vp, C.POINTER(C.c_uint64)]
+        L.wrt_measure_smem_bandwidth.argtypes = [_vp, C.POINTER(C.c_double)]
+        L.wrt_device_alloc.argtypes = [_vp, _sz, C.POINTER(_vp)]
+        L.wrt_device_free.argtypes = [_vp, _vp]
+        L.wrt_host_alloc_pinned.argtypes = [_vp, _sz, C.POINTER(_vp)]
+        L.wrt_host_free_pinned.argtypes = [_vp, _vp]
+        L.wrt_copy_to_device.argtypes = [_vp, _vp, _vp, _sz]
+        L.wrt_copy_to_host.argtypes = [_vp, _vp, _vp, _sz]
         _lib = L
     return _lib
 
@@ -149,6 +161,31 @@ class Context:
     def synchronize(self):
         self.check(lib().wrt_ctx_synchronize(self._h), "synchronize")
 
+    # -- measurement
+    def timer_start(self):
+        self.check(lib().wrt_ctx_timer_start(self._h), "timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        self.check(lib().wrt_ctx_timer_stop(self._h, C.byref(ms)), "timer_stop")
+        return float(ms.value)
+
+    def flush_l2(self):
+        self.check(lib().wrt_ctx_flush_l2(self._h), "flush_l2")
+
+    def count_samples(self, on: bool):
+        self.check(lib().wrt_ctx_count_samples(self._h, int(bool(on))), "count_samples")
+
+    def sample_count(self) -> int:
+        v = C.c_uint64()
+        self.check(lib().wrt_ctx_sample_count(self._h, C.byref(v)), "sample_count")
+        return int(v.value)
+
+    def smem_bandwidth(self) -> float:
+        v = C.c_double()
+        self.check(lib().wrt_measure_smem_bandwidth(self._h, C.byref(v)), "smem_bandwidth")
+        return float(v.value)
+
     # -- grids
     def gauss_legendre(self, n: int):
         x, w = np.empty(n), np.empty(n)
@@ -205,3 +242,133 @@ class Context:
         self.check(lib().wrt_radon_transpose(self._h, g, ngrid, nphi, ntheta, nshift, C.byref(o),
                                              out), "radon_transpose")
         return out
+
+
+class DeviceBuffer:
+    """Caller-owned device memory (wrt_device_alloc), counted in the budget."""
+
+    def __init__(self, ctx: Context, nbytes: int):
+        self.ctx, self.nbytes, self._p = ctx, int(nbytes), _vp()
+        ctx.check(lib().wrt_device_alloc(ctx.handle, self.nbytes, C.byref(self._p)), "device_alloc")
+
+    @property
+    def ptr(self) -> int:
+        return int(self._p.value)
+
+    def upload(self, host: np.ndarray):
+        a = np.ascontiguousarray(host)
+        assert a.nbytes <= self.nbytes
+        self.ctx.check(lib().wrt_copy_to_device(self.ctx.handle, self._p, a.ctypes.data_as(_vp),
+                                                a.nbytes), "copy_to_device")
+
+    def download(self, out: np.ndarray) -> np.ndarray:
+        assert out.flags.c_contiguous and out.nbytes <= self.nbytes
+        self.ctx.check(lib().wrt_copy_to_host(self.ctx.handle, out.ctypes.data_as(_vp), self._p,
+                                              out.nbytes), "copy_to_host")
+        return out
+
+    def close(self):
+        if self._p:
+            lib().wrt_device_free(self.ctx.handle, self._p)
+            self._p = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PinnedArray:
+    """A numpy array over page-locked host memory (wrt_host_alloc_pinned)."""
+
+    def __init__(self, ctx: Context, shape, dtype=np.float64):
+        self.ctx, self._p = ctx, _vp()
+        dt = np.dtype(dtype)
+        nbytes = int(np.prod(shape)) * dt.itemsize
+        ctx.check(lib().wrt_host_alloc_pinned(ctx.handle, nbytes, C.byref(self._p)), "pinned")
+        buf = (C.c_char * nbytes).from_address(self._p.value)
+        self.array = np.frombuffer(buf, dtype=dt).reshape(shape)
+
+    def close(self):
+        if self._p:
+            self.array = None
+            lib().wrt_host_free_pinned(self.ctx.handle, self._p)
+            self._p = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Volume:
+    """A volume resident on the device (wrt_volume)."""
+
+    def __init__(self, ctx: Context, n: int):
+        self.ctx, self.n, self._h = ctx, int(n), _vp()
+        ctx.check(lib().wrt_volume_create(ctx.handle, self.n, C.byref(self._h)), "volume_create")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def upload(self, data):
+        a = np.ascontiguousarray(data)
+        if a.shape != (self.n,) * 3:
+            raise ValueError(f"volume must be {(self.n,) * 3}, got {a.shape}")
+        if a.dtype == np.float32:
+            st = lib().wrt_volume_upload(self._h, None, a.ctypes.data_as(_vp))
+        else:
+            a = a.astype(np.float64, copy=False)
+            st = lib().wrt_volume_upload(self._h, a.ctypes.data_as(_vp), None)
+        self.ctx.check(st, "volume_upload")
+
+    def close(self):
+        if self._h:
+            lib().wrt_volume_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Grid:
+    """A Gauss-uniform sphere grid with its tables resident on the device."""
+
+    def __init__(self, ctx: Context, nphi: int, ntheta: int, nshift: int):
+        self.ctx, self._h = ctx, _vp()
+        self.nphi, self.ntheta, self.nshift = int(nphi), int(ntheta), int(nshift)
+        ctx.check(lib().wrt_grid_create(ctx.handle, self.nphi, self.ntheta, self.nshift,
+                                        C.byref(self._h)), "grid_create")
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def nplanes(self) -> int:
+        return self.nphi * self.ntheta * self.nshift
+
+    def close(self):
+        if self._h:
+            lib().wrt_grid_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def radon_forward_device(ctx: Context, vol: Volume, grid: Grid, dev_out: int, sampler=TRILINEAR,
+                         half_extent=0, kernel=KERNEL_AUTO):
+    """Plane integrals of a resident volume into device memory at ``dev_out``."""
+    o = plane_opts(sampler, half_extent, kernel)
+    ctx.check(lib().wrt_radon_forward_device(ctx.handle, vol.handle, grid.handle, C.byref(o),
+                                             _vp(dev_out)), "radon_forward_device")

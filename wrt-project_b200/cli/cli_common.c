@@ -1,0 +1,286 @@
+/* cli_common.c -- argument parsing, text I/O and a parallel formatter for the
+ * drop-in programs.  See cli_common.h for the contract. */
+#define _GNU_SOURCE
+#include "cli_common.h"
+
+#include <errno.h>
+#include <getopt.h>
+#include <pthread.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+double cli_now(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return t.tv_sec + 1e-9 * t.tv_nsec;
+}
+
+static void usage_exit(const char *prog, const char *usage, FILE *s, int code) {
+  fprintf(s, "Usage: %s %s\n", prog, usage);
+  fprintf(s,
+          "   -h --help                 Display this usage information.\n"
+          "   -p --parameters filename  Read the grid parameters from file.\n"
+          "   -i --input filename       Read input data from file.\n"
+          "   -o --output filename      Write output data to the file.\n"
+          "   -n --nthreads number      Number of host threads (text formatting).\n"
+          "      --device N             CUDA device ordinal (default 0).\n"
+          "      --binary               Also write OUTPUT.bin (raw FP64 results).\n");
+  exit(code);
+}
+
+void cli_parse(int argc, char **argv, cli_args *a, const char *usage, int allow_small,
+               int allow_sampler) {
+  memset(a, 0, sizeof(*a));
+  a->nthreads = 1;
+  a->sampler = WRT_SAMPLER_NEAREST;
+  if (argc == 1) {
+    fprintf(stderr, "%s: arguments required. Try '-h' or '--help'.\n", argv[0]);
+    exit(EXIT_FAILURE);
+  }
+  enum { OPT_DEVICE = 1000, OPT_BINARY, OPT_SAMPLER, OPT_HALF };
+  const struct option longopts[] = {
+      {"help", no_argument, 0, 'h'},          {"parameters", required_argument, 0, 'p'},
+      {"input", required_argument, 0, 'i'},   {"output", required_argument, 0, 'o'},
+      {"nthreads", required_argument, 0, 'n'}, {"small", no_argument, 0, 's'},
+      {"device", required_argument, 0, OPT_DEVICE}, {"binary", no_argument, 0, OPT_BINARY},
+      {"sampler", required_argument, 0, OPT_SAMPLER},
+      {"half-extent", required_argument, 0, OPT_HALF}, {0, 0, 0, 0}};
+  const char *shortopts = allow_small ? "hp:i:so:n:" : "hp:i:o:n:";
+  int c;
+  while ((c = getopt_long(argc, argv, shortopts, longopts, NULL)) != -1) {
+    switch (c) {
+      case 'h': usage_exit(argv[0], usage, stdout, 0); break;
+      case 'p': a->params = optarg; printf("Parameters file: %s\n", optarg); break;
+      case 'i': a->input = optarg; printf("Input file: %s\n", optarg); break;
+      case 'o': a->output = optarg; printf("Output file: %s\n", optarg); break;
+      case 'n':
+        a->nthreads = atoi(optarg);
+        if (a->nthreads <= 0) {
+          fprintf(stderr, "%s: -n expects a positive number\n", argv[0]);
+          exit(EXIT_FAILURE);
+        }
+        printf("Number of threads: %d\n", a->nthreads);
+        break;
+      case 's':
+        if (!allow_small) usage_exit(argv[0], usage, stderr, 1);
+        a->small_format = 1;
+        printf("Reading of the input in small format\n");
+        break;
+      case OPT_DEVICE: a->device = atoi(optarg); break;
+      case OPT_BINARY: a->binary = 1; break;
+      case OPT_SAMPLER:
+        if (!allow_sampler) usage_exit(argv[0], usage, stderr, 1);
+        if (!strcmp(optarg, "nearest")) a->sampler = WRT_SAMPLER_NEAREST;
+        else if (!strcmp(optarg, "trilinear")) a->sampler = WRT_SAMPLER_TRILINEAR;
+        else usage_exit(argv[0], usage, stderr, 1);
+        break;
+      case OPT_HALF:
+        if (!allow_sampler) usage_exit(argv[0], usage, stderr, 1);
+        a->half_extent = atoi(optarg);
+        break;
+      default: usage_exit(argv[0], usage, stderr, 1);
+    }
+  }
+  if (optind < argc) printf("Warning: non-option ARGV-arguments are omitted. See '-h' or '--help'.\n");
+  if (!a->params || !a->input || !a->output) {
+    fprintf(stderr, "%s: -p, -i and -o are required. Try '-h' or '--help'.\n", argv[0]);
+    exit(EXIT_FAILURE);
+  }
+}
+
+int cli_read_params(const char *path, int p[4]) {
+  FILE *f = fopen(path, "r");
+  if (!f) {
+    fprintf(stderr, "Recieved call %s while opening %s. \n", strerror(errno), path);
+    return -1;
+  }
+  char buffer[4096];
+  for (int k = 0; k < 4; ++k) {
+    int count = fscanf(f, "%d %4095[^\n]\n", &p[k], buffer);
+    if (count == EOF) {
+      fprintf(stderr, "Error: fscanf parameters %d : reached end of file before it was expected.\n", k);
+      fclose(f);
+      return -1;
+    } else if (count != 2) {
+      fprintf(stderr, "Error: fscanf parameters %d : matching failure, fscanf expected 1 integer value.\n", k);
+      fclose(f);
+      return -1;
+    }
+  }
+  fclose(f);
+  return 0;
+}
+
+/* Whole-file read; returns a NUL-terminated buffer or NULL. */
+static char *slurp(const char *path, size_t *len) {
+  FILE *f = fopen(path, "rb");
+  if (!f) {
+    fprintf(stderr, "Recieved call %s while opening %s. \n", strerror(errno), path);
+    return NULL;
+  }
+  fseek(f, 0, SEEK_END);
+  long n = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  char *buf = malloc((size_t)n + 1);
+  if (!buf || fread(buf, 1, (size_t)n, f) != (size_t)n) {
+    fprintf(stderr, "Error: could not read %s\n", path);
+    free(buf);
+    fclose(f);
+    return NULL;
+  }
+  buf[n] = 0;
+  fclose(f);
+  *len = (size_t)n;
+  return buf;
+}
+
+static int parse_values(const char *path, size_t count, double *out, int columns) {
+  size_t len = 0;
+  char *buf = slurp(path, &len);
+  if (!buf) return -1;
+  char *p = buf;
+  for (size_t k = 0; k < count; ++k) {
+    double v = 0;
+    for (int c = 0; c < columns; ++c) {
+      char *end;
+      v = strtod(p, &end);
+      if (end == p) {
+        fprintf(stderr,
+                *p ? "Error: %s: matching failure at value %zu, expected %d floating-point value(s).\n"
+                   : "Error: %s: reached the end of file before it was expected (value %zu of %d-column data).\n",
+                path, k, columns);
+        free(buf);
+        return -1;
+      }
+      p = end;
+      while (*p == ' ' || *p == '\t') ++p;
+      if (c + 1 < columns) {
+        if (*p != ',') {
+          fprintf(stderr, "Error: %s: matching failure at line %zu, expected %d columns.\n", path, k, columns);
+          free(buf);
+          return -1;
+        }
+        ++p;
+      }
+    }
+    out[k] = v;
+    while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n') ++p;
+  }
+  free(buf);
+  return 0;
+}
+
+int cli_read_column(const char *path, size_t count, double *out) {
+  return parse_values(path, count, out, 1);
+}
+
+int cli_read_csv4(const char *path, size_t count, double *out) {
+  return parse_values(path, count, out, 4);
+}
+
+typedef struct {
+  size_t lo, hi;
+  cli_row_fn row;
+  const void *ctx;
+  char *buf;
+  size_t len;
+} fmt_job;
+
+static void *fmt_worker(void *arg) {
+  fmt_job *j = arg;
+  size_t cap = (j->hi - j->lo) * 64 + 64, len = 0;
+  j->buf = malloc(cap);
+  for (size_t k = j->lo; k < j->hi && j->buf; ++k) {
+    if (cap - len < 256) {
+      cap *= 2;
+      char *nb = realloc(j->buf, cap);
+      if (!nb) {
+        free(j->buf);
+        j->buf = NULL;
+        break;
+      }
+      j->buf = nb;
+    }
+    len += (size_t)j->row(j->buf + len, k, j->ctx);
+  }
+  j->len = len;
+  return NULL;
+}
+
+int cli_write_rows(const char *path, size_t count, cli_row_fn row, const void *ctx, int nthreads) {
+  FILE *f = fopen(path, "w");
+  if (!f) {
+    fprintf(stderr, "Recieved call %s while opening %s. \n", strerror(errno), path);
+    return -1;
+  }
+  if (nthreads < 1) nthreads = 1;
+  const size_t block = 1 << 18;  /* rows per formatting job */
+  int rc = 0;
+  for (size_t base = 0; base < count && !rc; base += block * (size_t)nthreads) {
+    fmt_job jobs[256];
+    pthread_t th[256];
+    int nj = 0;
+    for (int t = 0; t < nthreads && t < 256; ++t) {
+      size_t lo = base + (size_t)t * block;
+      if (lo >= count) break;
+      size_t hi = lo + block < count ? lo + block : count;
+      jobs[nj] = (fmt_job){lo, hi, row, ctx, NULL, 0};
+      if (nthreads == 1 || pthread_create(&th[nj], NULL, fmt_worker, &jobs[nj]) != 0) {
+        fmt_worker(&jobs[nj]);
+        th[nj] = 0;
+      }
+      ++nj;
+    }
+    for (int t = 0; t < nj; ++t) {
+      if (th[t]) pthread_join(th[t], NULL);
+      if (!jobs[t].buf || fwrite(jobs[t].buf, 1, jobs[t].len, f) != jobs[t].len) rc = -1;
+      free(jobs[t].buf);
+    }
+  }
+  if (fclose(f) != 0) rc = -1;
+  if (rc) fprintf(stderr, "Error: failed writing %s\n", path);
+  return rc;
+}
+
+int cli_write_binary(const char *path, const double *v, size_t count) {
+  char name[4096];
+  snprintf(name, sizeof(name), "%s.bin", path);
+  FILE *f = fopen(name, "wb");
+  if (!f) return -1;
+  size_t w = fwrite(v, sizeof(double), count, f);
+  fclose(f);
+  return w == count ? 0 : -1;
+}
+
+void cli_readme(const char *output, const char *fmt, ...) {
+  char name[4096];
+  snprintf(name, sizeof(name), "readme_%s", output);
+  FILE *f = fopen(name, "w");
+  if (!f) {
+    fprintf(stderr, "Warning: could not write %s\n", name);
+    return;
+  }
+  va_list ap;
+  va_start(ap, fmt);
+  vfprintf(f, fmt, ap);
+  va_end(ap);
+  fclose(f);
+}
+
+wrt_ctx *cli_context(const cli_args *a) {
+  wrt_ctx *ctx = NULL;
+  int st = wrt_ctx_create(a->device, 0, &ctx);
+  if (st) {
+    fprintf(stderr, "Aborting : no CUDA context on device %d: %s\n", a->device, wrt_status_string(st));
+    exit(EXIT_FAILURE);
+  }
+  return ctx;
+}
+
+void cli_die_status(wrt_ctx *ctx, int st, const char *what) {
+  if (!st) return;
+  fprintf(stderr, "Aborting : %s: %s (%s)\n", what, wrt_status_string(st), wrt_ctx_last_error(ctx));
+  exit(EXIT_FAILURE);
+}

@@ -192,6 +192,11 @@ int wrt_ctx_destroy(wrt_ctx *ctx) {
   if (!ctx) return WRT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  ctx_free(ctx, ctx->flush_buf, ctx->flush_bytes);
+  ctx_free(ctx, ctx->d_counter, sizeof(unsigned long long));
+  for (auto &kv : ctx->user_allocs) cudaFree(kv.first);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WRT_OK;
@@ -206,6 +211,112 @@ int wrt_ctx_synchronize(wrt_ctx *ctx) {
 }
 
 size_t wrt_ctx_bytes_in_use(const wrt_ctx *ctx) { return ctx ? ctx->in_use : 0; }
+
+int wrt_ctx_timer_start(wrt_ctx *ctx) {
+  if (!ctx) return WRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->ev_start && (cudaEventCreate(&ctx->ev_start) != cudaSuccess ||
+                         cudaEventCreate(&ctx->ev_stop) != cudaSuccess))
+    return fail(ctx, WRT_ERR_CUDA, "timer events");
+  cudaError_t e = cudaEventRecord(ctx->ev_start, ctx->stream);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, "timer start");
+}
+
+int wrt_ctx_timer_stop(wrt_ctx *ctx, float *ms) {
+  if (!ctx || !ms || !ctx->ev_start) return WRT_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaEventRecord(ctx->ev_stop, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ctx->ev_stop);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, ctx->ev_start, ctx->ev_stop);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, "timer stop");
+}
+
+int wrt_ctx_flush_l2(wrt_ctx *ctx) {
+  if (!ctx) return WRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->flush_buf) {
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device);
+    const size_t bytes = 2 * (size_t)(l2 > 0 ? l2 : (128 << 20));
+    int st = ctx_alloc(ctx, &ctx->flush_buf, bytes);
+    if (st) return st;
+    ctx->flush_bytes = bytes;
+  }
+  cudaError_t e = cudaMemsetAsync(ctx->flush_buf, ctx->launches & 0xff, ctx->flush_bytes, ctx->stream);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, "flush l2");
+}
+
+int wrt_ctx_count_samples(wrt_ctx *ctx, int on) {
+  if (!ctx) return WRT_ERR_INVALID_ARGUMENT;
+  if (on && !ctx->d_counter) {
+    int st = ctx_alloc(ctx, (void **)&ctx->d_counter, sizeof(unsigned long long));
+    if (st) return st;
+    cudaError_t e = cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sample counter");
+  } else if (!on && ctx->d_counter) {
+    cudaStreamSynchronize(ctx->stream);
+    ctx_free(ctx, ctx->d_counter, sizeof(unsigned long long));
+    ctx->d_counter = nullptr;
+  }
+  return WRT_OK;
+}
+
+int wrt_ctx_sample_count(wrt_ctx *ctx, uint64_t *count) {
+  if (!ctx || !count) return WRT_ERR_INVALID_ARGUMENT;
+  *count = 0;
+  if (!ctx->d_counter) return WRT_OK;
+  unsigned long long v = 0;
+  int st = d2h_sync(ctx, &v, ctx->d_counter, sizeof(v), "sample count");
+  if (!st) *count = v;
+  return st;
+}
+
+int wrt_device_alloc(wrt_ctx *ctx, size_t bytes, void **dev_ptr) {
+  if (!ctx || !dev_ptr || bytes == 0) return WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  if (!st) st = ctx_alloc(ctx, dev_ptr, bytes);
+  if (!st) ctx->user_allocs[*dev_ptr] = bytes;
+  return st;
+}
+
+int wrt_device_free(wrt_ctx *ctx, void *p) {
+  if (!ctx || !p) return WRT_ERR_INVALID_ARGUMENT;
+  auto it = ctx->user_allocs.find(p);
+  if (it == ctx->user_allocs.end()) return fail(ctx, WRT_ERR_NOT_FOUND, "unknown device pointer");
+  cudaStreamSynchronize(ctx->stream);
+  ctx_free(ctx, p, it->second);
+  ctx->user_allocs.erase(it);
+  return WRT_OK;
+}
+
+int wrt_host_alloc_pinned(wrt_ctx *ctx, size_t bytes, void **host_ptr) {
+  if (!ctx || !host_ptr || bytes == 0) return WRT_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaMallocHost(host_ptr, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, WRT_ERR_OUT_OF_MEMORY, "cudaMallocHost(%zu)", bytes);
+  }
+  return WRT_OK;
+}
+
+int wrt_host_free_pinned(wrt_ctx *ctx, void *host_ptr) {
+  if (!ctx || !host_ptr) return WRT_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaFreeHost(host_ptr);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, "cudaFreeHost");
+}
+
+int wrt_copy_to_device(wrt_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  if (!ctx || !dst || !src) return WRT_ERR_INVALID_ARGUMENT;
+  return h2d(ctx, dst, src, bytes, "copy to device");
+}
+
+int wrt_copy_to_host(wrt_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  if (!ctx || !dst || !src) return WRT_ERR_INVALID_ARGUMENT;
+  return d2h_sync(ctx, dst, src, bytes, "copy to host");
+}
+
+int wrt_measure_smem_bandwidth(wrt_ctx *ctx, double *bytes_per_s) {
+  if (!ctx || !bytes_per_s) return WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  return st ? st : smem_bandwidth(ctx, bytes_per_s);
+}
 uint64_t wrt_ctx_launch_count(const wrt_ctx *ctx) { return ctx ? ctx->launches : 0; }
 void *wrt_ctx_stream(wrt_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
@@ -356,6 +467,7 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid
   job.r2bits = vol->d_r2;
   job.margin = sampler_margin(vol->n, o.sampler);
   job.out = dev_out;
+  job.counter = ctx->d_counter;
   return plane_forward_plain(ctx, job);
 }
 

@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(256) plane_plain_kernel(wrt::PlaneJob job, flo
   const int n = job.n;
   const PlaneConsts c = plane_consts(job, is, d);
   double acc = 0.0;
+  int evaluated = 0;
   if (c.rem >= 0.0) {
     // cells per unit length of the sampler's grid
     const double h = SAMPLER == WRT_SAMPLER_TRILINEAR ? 0.5 * (n - 1) : 0.5 * n;
@@ -130,8 +131,10 @@ __global__ void __launch_bounds__(256) plane_plain_kernel(wrt::PlaneJob job, flo
             const double pz = __dadd_rn(r.bz, __dmul_rn(c.a2z, dj));
             acc += SAMPLER == WRT_SAMPLER_TRILINEAR ? wrtd::exact_trilinear(job.vol, n, px, py, pz)
                                                     : wrtd::exact_nearest(job.vol, n, px, py, pz);
+            ++evaluated;
           } else if (qx > 0.0f && qy > 0.0f && qz > 0.0f && qx < qmax && qy < qmax &&
                      qz < qmax) {
+            ++evaluated;
             if (SAMPLER == WRT_SAMPLER_TRILINEAR) {
               part += wrtd::tri32(job.vol, n, qx, qy, qz);
             } else {
@@ -145,6 +148,10 @@ __global__ void __launch_bounds__(256) plane_plain_kernel(wrt::PlaneJob job, flo
   }
   acc = wrtd::warp_sum(acc);
   if (lane == 0) job.out[plane] = acc * c.delta * c.delta;
+  if (job.counter) {
+    for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
+    if (lane == 0) atomicAdd(job.counter, (unsigned long long)evaluated);
+  }
 }
 
 // Exact transpose: every sample of every plane scatters g[plane] * delta^2 *

@@ -24,6 +24,8 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <unordered_map>
+
 #include "../../include/wrt.h"
 
 #define WRT_PI 3.14159265358979323846
@@ -37,6 +39,12 @@ struct wrt_ctx {
   cudaStream_t stream = nullptr;
   int sm_count = 0;
   char err[512] = {0};
+  // measurement helpers (api.cu)
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  void *flush_buf = nullptr;
+  size_t flush_bytes = 0;
+  unsigned long long *d_counter = nullptr;  // non-null while counting samples
+  std::unordered_map<void *, size_t> user_allocs;  // wrt_device_alloc sizes
 };
 
 namespace wrt {
@@ -77,6 +85,7 @@ struct PlaneJob {
   const unsigned int *r2bits;  // device: largest |x|^2 of a non-zero node (float bits)
   double margin;         // crop radius = sqrt(r2) + margin (>= the sampler's reach)
   double *out;           // [nshift][ndir]
+  unsigned long long *counter;  // optional: samples evaluated
 };
 int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job);
 int plane_transpose(wrt_ctx *ctx, const PlaneJob &job, const double *d_g, double *d_vol64);
@@ -94,6 +103,9 @@ struct RayJob {
   double *out;          // [nslices][nshift][nphi]
 };
 int ray_forward(wrt_ctx *ctx, const RayJob &job);
+
+// Shared-memory bandwidth microbenchmark (k_probe.cu).
+int smem_bandwidth(wrt_ctx *ctx, double *bytes_per_s);
 
 // Spline / reduction / adjoint kernels (k_spline.cu).
 int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_ray,
