@@ -109,3 +109,46 @@ def test_transpose_inner_product(ctx, vol24, sampler):
     assert abs(lhs - rhs) <= 1e-6 * max(abs(lhs), abs(rhs))
     ref = O.radon_transpose(g, 24, sampler=sampler)
     assert rel_l2(RTg, ref) < TOL_L2
+
+
+# ----------------------------------------------------------- staged kernel
+STAGED_CASES = [
+    (24, (16, 8, 12), 0),     # one tile, the reference's lattice [-2n, 2n)^2
+    (24, (12, 6, 10), 24),    # lattice [-n, n)^2 (the benchmark's definition)
+    (33, (9, 7, 13), 0),      # odd n: z = 0 is a node (guard-band rows)
+    (64, (16, 8, 20), 64),
+    (200, (6, 4, 7), 200),    # several y-tiles
+]
+
+
+@pytest.mark.parametrize("n,grid,L", STAGED_CASES)
+def test_staged_matches_oracle(ctx, n, grid, L):
+    vol = ellipsoid_phantom(n, 8, 2000 + n)
+    got = ctx.radon_grid(vol, *grid, sampler=O.TRILINEAR, half_extent=L, kernel=wrt.KERNEL_STAGED)
+    ref = O.radon_forward(vol, *grid, sampler=O.TRILINEAR, half_extent=L)
+    assert rel_l2(got, ref) < TOL_L2
+    assert rel_max(got, ref) < 1e-4
+
+
+def test_staged_random_volume_nonzero_faces(ctx, volrand):
+    got = ctx.radon_grid(volrand, 8, 6, 9, sampler=O.TRILINEAR, kernel=wrt.KERNEL_STAGED)
+    ref = O.radon_forward(volrand, 8, 6, 9, sampler=O.TRILINEAR)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+def test_staged_is_bitwise_deterministic(ctx, vol24):
+    a = ctx.radon_grid(vol24, 16, 8, 12, sampler=O.TRILINEAR, kernel=wrt.KERNEL_STAGED)
+    b = ctx.radon_grid(vol24, 16, 8, 12, sampler=O.TRILINEAR, kernel=wrt.KERNEL_STAGED)
+    assert np.array_equal(a, b)
+
+
+def test_staged_agrees_with_plain(ctx):
+    vol = ellipsoid_phantom(48, 10, 4242)
+    a = ctx.radon_grid(vol, 24, 12, 33, sampler=O.TRILINEAR, half_extent=48, kernel=wrt.KERNEL_STAGED)
+    b = ctx.radon_grid(vol, 24, 12, 33, sampler=O.TRILINEAR, half_extent=48, kernel=wrt.KERNEL_PLAIN)
+    assert rel_l2(a, b) < 2e-6
+
+
+def test_staged_rejects_nearest(ctx, vol24):
+    with pytest.raises(wrt.WrtError):
+        ctx.radon_grid(vol24, 4, 4, 4, sampler=O.NEAREST, kernel=wrt.KERNEL_STAGED)

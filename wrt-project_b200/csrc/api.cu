@@ -21,8 +21,9 @@ struct wrt_volume {
   wrt_ctx *ctx = nullptr;
   int n = 0;
   float *d_vol = nullptr;          // n^3, v[ix][iy][iz]
-  unsigned int *d_r2 = nullptr;    // largest |x|^2 of a non-zero node (float bits)
-  float2 *d_pairs = nullptr;       // layer pairs for the staged kernel (lazy)
+  unsigned int *d_stats = nullptr; // [0] largest |x|^2 of a non-zero node, [1] max |v| (float bits)
+  float r2 = 3.0f, maxabs = 0.0f;  // host copies of d_stats, read at upload
+  float2 *d_pairs = nullptr;       // layer pairs for the staged kernel (built on first use)
   int pitch = 0;
   size_t vol_bytes = 0, pair_bytes = 0;
   bool pairs_valid = false;
@@ -34,6 +35,8 @@ struct wrt_grid {
   std::vector<double> phi, theta, w, shift;
   double *d_dir = nullptr;    // [nphi*ntheta][9]
   double *d_shift = nullptr;  // [nshift]
+  float *d_dir32 = nullptr;   // [nphi*ntheta][8]
+  float *d_shift32 = nullptr; // [nshift]
   size_t bytes = 0;
 };
 
@@ -197,6 +200,7 @@ int wrt_ctx_destroy(wrt_ctx *ctx) {
   ctx_free(ctx, ctx->flush_buf, ctx->flush_bytes);
   ctx_free(ctx, ctx->d_counter, sizeof(unsigned long long));
   for (auto &kv : ctx->user_allocs) cudaFree(kv.first);
+  staged_release(ctx);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WRT_OK;
@@ -345,7 +349,7 @@ int wrt_volume_create(wrt_ctx *ctx, int n, wrt_volume **out) {
   v->n = n;
   v->vol_bytes = sizeof(float) * (size_t)n * n * n;
   st = ctx_alloc(ctx, (void **)&v->d_vol, v->vol_bytes);
-  if (!st) st = ctx_alloc(ctx, (void **)&v->d_r2, sizeof(unsigned int));
+  if (!st) st = ctx_alloc(ctx, (void **)&v->d_stats, 2 * sizeof(unsigned int));
   if (st) {
     wrt_volume_destroy(v);
     return st;
@@ -353,6 +357,34 @@ int wrt_volume_create(wrt_ctx *ctx, int n, wrt_volume **out) {
   *out = v;
   return WRT_OK;
 }
+
+namespace {
+// Waits for the upload and copies the volume statistics to the host.
+int volume_finish_upload(wrt_volume *v) {
+  wrt_ctx *ctx = v->ctx;
+  unsigned int stats[2] = {0, 0};
+  int st = d2h_sync(ctx, stats, v->d_stats, sizeof(stats), "volume statistics");
+  if (st) return st;
+  memcpy(&v->r2, &stats[0], sizeof(float));
+  memcpy(&v->maxabs, &stats[1], sizeof(float));
+  v->pairs_valid = false;
+  return WRT_OK;
+}
+
+int volume_ensure_pairs(wrt_volume *v) {
+  if (v->pairs_valid) return WRT_OK;
+  wrt_ctx *ctx = v->ctx;
+  if (!v->d_pairs) {
+    v->pitch = v->n + (v->n & 1);
+    v->pair_bytes = sizeof(float2) * (size_t)(v->n - 1) * v->n * v->pitch;
+    int st = ctx_alloc(ctx, (void **)&v->d_pairs, v->pair_bytes);
+    if (st) return st;
+  }
+  int st = volume_pairs(ctx, v->d_vol, v->n, v->d_pairs, v->pitch);
+  if (!st) v->pairs_valid = true;
+  return st;
+}
+}  // namespace
 
 int wrt_volume_upload(wrt_volume *v, const double *f64, const float *f32) {
   if (!v || ((f64 == nullptr) == (f32 == nullptr))) return WRT_ERR_INVALID_ARGUMENT;
@@ -364,13 +396,9 @@ int wrt_volume_upload(wrt_volume *v, const double *f64, const float *f32) {
   st = stage.alloc(count * (f64 ? sizeof(double) : sizeof(float)));
   if (!st) st = h2d(ctx, stage.p, f64 ? (const void *)f64 : (const void *)f32, stage.bytes, "volume upload");
   if (!st)
-    st = f64 ? volume_from_f64(ctx, stage.as<double>(), v->n, v->d_vol, v->d_r2)
-             : volume_from_f32(ctx, stage.as<float>(), v->n, v->d_vol, v->d_r2);
-  if (!st) {
-    cudaError_t e = cudaStreamSynchronize(ctx->stream);  // the staging buffer dies here
-    if (e != cudaSuccess) st = cuda_fail(ctx, e, "volume upload");
-  }
-  v->pairs_valid = false;
+    st = f64 ? volume_from_f64(ctx, stage.as<double>(), v->n, v->d_vol, v->d_stats)
+             : volume_from_f32(ctx, stage.as<float>(), v->n, v->d_vol, v->d_stats);
+  if (!st) st = volume_finish_upload(v);  // also keeps the staging buffer alive until done
   return st;
 }
 
@@ -378,8 +406,8 @@ int wrt_volume_upload_device(wrt_volume *v, const float *dev_f32) {
   if (!v || !dev_f32) return WRT_ERR_INVALID_ARGUMENT;
   int st = set_device(v->ctx);
   if (st) return st;
-  st = volume_from_f32(v->ctx, dev_f32, v->n, v->d_vol, v->d_r2);
-  v->pairs_valid = false;
+  st = volume_from_f32(v->ctx, dev_f32, v->n, v->d_vol, v->d_stats);
+  if (!st) st = volume_finish_upload(v);
   return st;
 }
 
@@ -389,7 +417,7 @@ int wrt_volume_destroy(wrt_volume *v) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx_free(ctx, v->d_vol, v->vol_bytes);
-  ctx_free(ctx, v->d_r2, sizeof(unsigned int));
+  ctx_free(ctx, v->d_stats, 2 * sizeof(unsigned int));
   ctx_free(ctx, v->d_pairs, v->pair_bytes);
   delete v;
   return WRT_OK;
@@ -415,14 +443,21 @@ int wrt_grid_create(wrt_ctx *ctx, int nphi, int ntheta, int nshift, wrt_grid **o
                    g->shift.data());
   const size_t ndir = (size_t)nphi * ntheta;
   std::vector<double> dir(ndir * 9);
+  std::vector<float> dir32(ndir * 8), shift32(nshift);
   if (!st) {
     plane_directions(nphi, g->phi.data(), ntheta, g->theta.data(), dir.data());
-    g->bytes = sizeof(double) * (dir.size() + nshift);
+    for (size_t d = 0; d < ndir; ++d)
+      for (int k = 0; k < 8; ++k) dir32[8 * d + k] = (float)dir[9 * d + k];
+    for (int i = 0; i < nshift; ++i) shift32[i] = (float)g->shift[i];
     st = ctx_alloc(ctx, (void **)&g->d_dir, sizeof(double) * dir.size());
   }
   if (!st) st = ctx_alloc(ctx, (void **)&g->d_shift, sizeof(double) * nshift);
+  if (!st) st = ctx_alloc(ctx, (void **)&g->d_dir32, sizeof(float) * dir32.size());
+  if (!st) st = ctx_alloc(ctx, (void **)&g->d_shift32, sizeof(float) * nshift);
   if (!st) st = h2d(ctx, g->d_dir, dir.data(), sizeof(double) * dir.size(), "grid upload");
   if (!st) st = h2d(ctx, g->d_shift, g->shift.data(), sizeof(double) * nshift, "grid upload");
+  if (!st) st = h2d(ctx, g->d_dir32, dir32.data(), sizeof(float) * dir32.size(), "grid upload");
+  if (!st) st = h2d(ctx, g->d_shift32, shift32.data(), sizeof(float) * nshift, "grid upload");
   if (!st) {
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) st = cuda_fail(ctx, e, "grid upload");
@@ -439,14 +474,69 @@ int wrt_grid_destroy(wrt_grid *g) {
   if (!g) return WRT_ERR_INVALID_ARGUMENT;
   cudaSetDevice(g->ctx->device);
   cudaStreamSynchronize(g->ctx->stream);
-  ctx_free(g->ctx, g->d_dir, sizeof(double) * 9 * (size_t)g->nphi * g->ntheta);
+  const size_t ndir = (size_t)g->nphi * g->ntheta;
+  ctx_free(g->ctx, g->d_dir, sizeof(double) * 9 * ndir);
   ctx_free(g->ctx, g->d_shift, sizeof(double) * g->nshift);
+  ctx_free(g->ctx, g->d_dir32, sizeof(float) * 8 * ndir);
+  ctx_free(g->ctx, g->d_shift32, sizeof(float) * g->nshift);
   delete g;
   return WRT_OK;
 }
 
-int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *grid,
+namespace {
+
+// Staged-kernel launch of one request; see k_staged.cu.
+int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, int L,
+                         double *dev_out) {
+  int st = volume_ensure_pairs(vol);
+  if (st) return st;
+  const int n = vol->n;
+  int th = 0, qp = 0;
+  const int smem = staged_smem_bytes(n, &th, &qp);
+  StagedReq r = {};
+  r.pairs = vol->d_pairs;
+  r.vol = vol->d_vol;
+  r.dir = grid->d_dir;
+  r.dir32 = grid->d_dir32;
+  r.shift = grid->d_shift;
+  r.shift32 = grid->d_shift32;
+  r.acc = reinterpret_cast<unsigned long long *>(dev_out);
+  r.n = n;
+  r.pitch2 = vol->pitch;
+  r.qpitch = qp;
+  r.tile_h = th;
+  r.ndir = grid->nphi * grid->ntheta;
+  r.nshift = grid->nshift;
+  r.L = L;
+  r.guard = 6.0e-7f * (float)(n > 64 ? n : 64);
+  const double rc = sqrt((double)vol->r2) + sampler_margin(n, WRT_SAMPLER_TRILINEAR);
+  r.crop_r2 = (float)fmin(rc * rc * (1.0 + 1e-6), 3.0 + 1e-5);
+  r.scale = fixed_point_scale(vol->maxabs, L);
+  StagedItem *d_items = nullptr;
+  int nitems = 0;
+  st = staged_items_cached(ctx, n, th, r.crop_r2, r.ndir, &d_items, &nitems);
+  if (st) return st;
+  st = staged_scratch(ctx, sizeof(StagedReq));
+  if (st) return st;
+  st = h2d(ctx, ctx->staged_req, &r, sizeof(r), "staged request");
+  if (st) return st;
+  const size_t nout = (size_t)r.ndir * r.nshift;
+  cudaError_t e = cudaMemsetAsync(dev_out, 0, sizeof(double) * nout, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "staged output reset");
+  if (nitems > 0) {
+    st = plane_staged_launch(ctx, (const StagedReq *)ctx->staged_req, d_items, nitems, smem,
+                             ctx->staged_next);
+    if (st) return st;
+  }
+  const double delta = 1.0 / n;
+  return plane_finalize(ctx, dev_out, (long long)nout, delta * delta / r.scale);
+}
+
+}  // namespace
+
+int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const wrt_grid *grid,
                              const wrt_plane_opts *opts, double *dev_out) {
+  wrt_volume *vol = const_cast<wrt_volume *>(cvol);
   if (!ctx || !vol || !grid || !dev_out || vol->ctx != ctx || grid->ctx != ctx)
     return WRT_ERR_INVALID_ARGUMENT;
   if (!valid_plane_opts(opts, vol->n))
@@ -455,6 +545,13 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid
   if (st) return st;
   wrt_plane_opts o = {};
   if (opts) o = *opts;
+  const int L = o.half_extent ? o.half_extent : 2 * vol->n;
+  int th = 0, qp = 0;
+  const bool staged_ok = o.sampler == WRT_SAMPLER_TRILINEAR && vol->n >= 4 &&
+                         staged_smem_bytes(vol->n, &th, &qp) > 0;
+  if (o.kernel == WRT_KERNEL_STAGED && !staged_ok)
+    return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "staged kernel needs the trilinear sampler");
+  if (o.kernel != WRT_KERNEL_PLAIN && staged_ok) return radon_forward_staged(ctx, vol, grid, L, dev_out);
   PlaneJob job = {};
   job.vol = vol->d_vol;
   job.n = vol->n;
@@ -462,9 +559,9 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid
   job.shift = grid->d_shift;
   job.ndir = grid->nphi * grid->ntheta;
   job.nshift = grid->nshift;
-  job.L = o.half_extent ? o.half_extent : 2 * vol->n;
+  job.L = L;
   job.sampler = o.sampler;
-  job.r2bits = vol->d_r2;
+  job.r2bits = vol->d_stats;
   job.margin = sampler_margin(vol->n, o.sampler);
   job.out = dev_out;
   job.counter = ctx->d_counter;
@@ -571,7 +668,7 @@ int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int n, int nslices, int nsh
     job.trig = dtrig.as<double>();
     job.shift = dshiftb.as<double>();
     job.frame = identity ? nullptr : dframe.as<double>();
-    job.r2bits = vol->d_r2;
+    job.r2bits = vol->d_stats;
     job.margin = sampler_margin(n, WRT_SAMPLER_TRILINEAR);
     job.out = dout.as<double>();
     st = ray_forward(ctx, job);

@@ -4,7 +4,9 @@
 // init.c:120-124), FP64 or FP32.  Output:
 //   * d_vol    FP32 copy in the same order (gathers of the plain kernels and
 //              the guard-band re-evaluation);
-//   * r2bits   the largest squared radius |x|^2 of a non-zero node, as the
+//   * stats[1] the largest |value| (float bits), which sizes the fixed-point
+//              accumulators of the staged kernel;
+//   * stats[0] the largest squared radius |x|^2 of a non-zero node, as the
 //              bit pattern of a non-negative float (monotone under integer
 //              max).  Every lattice sample farther than sqrt(r2) + sqrt(3)
 //              delta from the origin has only zero corners, so it contributes
@@ -19,14 +21,15 @@ namespace {
 
 template <typename T>
 __global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *__restrict__ dst,
-                                      unsigned int *__restrict__ r2bits) {
+                                      unsigned int *__restrict__ stats) {
   const size_t total = (size_t)n * n * n;
   const double h = 2.0 / (n - 1);
-  float local = 0.0f;
+  float local = 0.0f, amax = 0.0f;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
        k += (size_t)gridDim.x * blockDim.x) {
     float v = (float)src[k];
     dst[k] = v;
+    amax = fmaxf(amax, fabsf(v));
     if (v != 0.0f) {
       int iz = (int)(k % n), iy = (int)((k / n) % n), ix = (int)(k / ((size_t)n * n));
       double x = -1.0 + h * ix, y = -1.0 + h * iy, z = -1.0 + h * iz;
@@ -35,8 +38,14 @@ __global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *_
     }
   }
   // warp max, one atomic per warp
-  for (int o = 16; o > 0; o >>= 1) local = fmaxf(local, __shfl_xor_sync(0xffffffffu, local, o));
-  if ((threadIdx.x & 31) == 0 && local > 0.0f) atomicMax(r2bits, __float_as_uint(local));
+  for (int o = 16; o > 0; o >>= 1) {
+    local = fmaxf(local, __shfl_xor_sync(0xffffffffu, local, o));
+    amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (local > 0.0f) atomicMax(stats, __float_as_uint(local));
+    if (amax > 0.0f) atomicMax(stats + 1, __float_as_uint(amax));
+  }
 }
 
 // pairs[iz][iy][ix] = (v[ix][iy][iz], v[ix][iy][iz+1]); one thread per output.
@@ -56,11 +65,11 @@ __global__ void volume_pairs_kernel(const float *__restrict__ v, int n, float2 *
 }
 
 template <typename T>
-int convert(wrt_ctx *ctx, const T *d_src, int n, float *d_vol, unsigned int *d_r2bits) {
-  cudaError_t e = cudaMemsetAsync(d_r2bits, 0, sizeof(unsigned int), ctx->stream);
-  if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "volume r2 reset");
+int convert(wrt_ctx *ctx, const T *d_src, int n, float *d_vol, unsigned int *d_stats) {
+  cudaError_t e = cudaMemsetAsync(d_stats, 0, 2 * sizeof(unsigned int), ctx->stream);
+  if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "volume stats reset");
   int blocks = ctx->sm_count * 8;
-  volume_convert_kernel<T><<<blocks, 256, 0, ctx->stream>>>(d_src, n, d_vol, d_r2bits);
+  volume_convert_kernel<T><<<blocks, 256, 0, ctx->stream>>>(d_src, n, d_vol, d_stats);
   ctx->launches++;
   return wrt::check_launch(ctx, "volume_convert_kernel");
 }

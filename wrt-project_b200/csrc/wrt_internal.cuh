@@ -25,6 +25,7 @@
 #include <stddef.h>
 
 #include <unordered_map>
+#include <vector>
 
 #include "../../include/wrt.h"
 
@@ -45,6 +46,12 @@ struct wrt_ctx {
   size_t flush_bytes = 0;
   unsigned long long *d_counter = nullptr;  // non-null while counting samples
   std::unordered_map<void *, size_t> user_allocs;  // wrt_device_alloc sizes
+  // staged plane kernel (k_staged.cu): request descriptors, item counter and
+  // the work-item lists of the geometries seen so far
+  void *staged_req = nullptr;
+  size_t staged_req_bytes = 0;
+  int *staged_next = nullptr;
+  void *staged_cache = nullptr;
 };
 
 namespace wrt {
@@ -66,10 +73,11 @@ int sphere_grid(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *phi,
 int gauss_legendre_device(wrt_ctx *ctx, int n, double *x_host, double *w_host);
 
 // Volume preparation kernels (k_volume.cu).
+// d_stats[0]: largest |x|^2 of a non-zero node, d_stats[1]: max |v| (float bits)
 int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
-                    unsigned int *d_r2bits);
+                    unsigned int *d_stats);
 int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
-                    unsigned int *d_r2bits);
+                    unsigned int *d_stats);
 int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch);
 
 // Plane kernels (k_plane.cu).
@@ -89,6 +97,34 @@ struct PlaneJob {
 };
 int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job);
 int plane_transpose(wrt_ctx *ctx, const PlaneJob &job, const double *d_g, double *d_vol64);
+
+// Staged plane kernel (k_staged.cu).
+struct StagedReq {
+  const float2 *pairs;     // layer pairs [iz][y][pitch2]
+  const float *vol;        // reference layout, for guard-band samples
+  const double *dir;       // [ndir][9] FP64 directions
+  const float *dir32;      // [ndir][8]: normal, v1, v2.x, v2.y (unscaled) FP32
+  const double *shift;     // [nshift]
+  const float *shift32;    // [nshift]
+  unsigned long long *acc; // [nshift][ndir] fixed-point accumulators (the output buffer)
+  int n, pitch2, qpitch, tile_h, ndir, nshift, L, pad;
+  float guard, crop_r2;
+  double scale;            // fixed-point scale 2^k
+};
+struct StagedItem {
+  int req, layer, tile, dir0, ndir;
+};
+int staged_smem_bytes(int n, int *tile_h, int *qpitch);
+int plane_staged_launch(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items,
+                        int nitems, int max_smem, int *d_next);
+int plane_finalize(wrt_ctx *ctx, double *out, long long count, double factor);
+void staged_items(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
+                  std::vector<StagedItem> &out);
+double fixed_point_scale(float maxabs, int L);
+int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir,
+                        StagedItem **d_items, int *nitems);
+int staged_scratch(wrt_ctx *ctx, size_t req_bytes);
+void staged_release(wrt_ctx *ctx);
 
 // Ray kernels (k_ray.cu).
 struct RayJob {
