@@ -105,14 +105,14 @@ def zero_interp(vol, x, y, z) -> float:
 def plane_integral(vol, phi, theta, shift, sampler=NEAREST, half_extent=None) -> float:
     v = _f64(vol)
     n = v.shape[0]
-    L = 2 * n if half_extent is None else half_extent
+    L = 2 * n if not half_extent else half_extent
     return _Lib.orc().orc_plane_integral(v, n, phi, theta, shift, sampler, L)
 
 
 def radon_forward(vol, nphi, ntheta, nshift, sampler=NEAREST, half_extent=None, nthreads=None):
     v = _f64(vol)
     n = v.shape[0]
-    L = 2 * n if half_extent is None else half_extent
+    L = 2 * n if not half_extent else half_extent
     out = np.empty((nshift, nphi, ntheta))
     _Lib.orc().orc_radon_forward(v, n, nphi, ntheta, nshift, sampler, L, out, _nthreads(nthreads))
     return out
@@ -121,7 +121,7 @@ def radon_forward(vol, nphi, ntheta, nshift, sampler=NEAREST, half_extent=None, 
 def radon_planes(vol, phi, theta, shift, sampler=NEAREST, half_extent=None, nthreads=None):
     v = _f64(vol)
     n = v.shape[0]
-    L = 2 * n if half_extent is None else half_extent
+    L = 2 * n if not half_extent else half_extent
     phi, theta, shift = _f64(phi), _f64(theta), _f64(shift)
     out = np.empty(phi.shape[0])
     _Lib.orc().orc_radon_planes(v, n, phi.shape[0], phi, theta, shift, sampler, L, out,
@@ -190,7 +190,7 @@ def adjoint_points(radon, x, y, z, nthreads=None):
 def radon_transpose(g, n, sampler=TRILINEAR, half_extent=None):
     g = _f64(g)
     nshift, nphi, ntheta = g.shape
-    L = 2 * n if half_extent is None else half_extent
+    L = 2 * n if not half_extent else half_extent
     out = np.zeros((n, n, n))
     _Lib.orc().orc_radon_transpose(g, n, nphi, ntheta, nshift, sampler, L, out)
     return out
