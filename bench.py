@@ -273,6 +273,15 @@ def run_ours(args, dist):
         wrt.radon_forward_device(ctx, vol, grid, out.ptr, sampler=wrt.TRILINEAR,
                                  half_extent=HALF_EXTENT, kernel=k)
 
+    # the autotuner picks the staged kernel's tile shape on this request
+    tile = None
+    if kernel != wrt.KERNEL_PLAIN:
+        best, best_ms = wrt.tune_plane_kernel(ctx, vol, grid, out.ptr, sampler=wrt.TRILINEAR,
+                                              half_extent=HALF_EXTENT)
+        t, g, s = wrt.plane_kernel_configs()[best]
+        tile = {"threads": t, "rows_per_warp_group": g, "shifts_per_lane": s,
+                "tuner_ms": best_ms}
+
     # samples evaluated per launch (one counted launch, outside the timed region)
     ctx.count_samples(True)
     step()
@@ -354,7 +363,7 @@ def run_ours(args, dist):
                                "64x128 Gauss-uniform sphere grid x 256 shifts, trilinear, "
                                "lattice step 1/n on [-n,n)^2",
                    "n": N, "sphere_grid": [NTHETA, NPHI], "shifts": NSHIFT,
-                   "planes_per_step": nplanes, "kernel": args.kernel,
+                   "planes_per_step": nplanes, "kernel": args.kernel, "tile": tile,
                    "l2": "flushed before every timed step (2x L2 memset)",
                    "parallelism": f"replicas x{dist.world}"},
         "samples_per_step": samples,

@@ -157,6 +157,20 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid
  * work against the library's. */
 void *wrt_ctx_stream(wrt_ctx *ctx);
 
+/* Autotuner of the staged plane kernel's tile shape (CTA size, lattice rows
+ * walked together per warp, shifts enumerated per lane): runs every
+ * configuration on this request (dev_out receives the result), times each
+ * with CUDA events and keeps the fastest in the context.  *best / *best_ms
+ * (either may be NULL) receive the chosen index and its time per launch. */
+int wrt_tune_plane_kernel(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *grid,
+                          const wrt_plane_opts *opts, double *dev_out, int *best,
+                          float *best_ms);
+/* Number of tile configurations; their shapes; force one (-1: default). */
+int wrt_plane_kernel_config_count(void);
+int wrt_plane_kernel_config_describe(int index, int *threads, int *rows_per_group,
+                                     int *shifts_per_lane);
+int wrt_ctx_set_plane_kernel_config(wrt_ctx *ctx, int index);
+
 /* Caller-owned device and pinned host memory, counted against the context's
  * budget (device) and released with the matching free. */
 int wrt_device_alloc(wrt_ctx *ctx, size_t bytes, void **dev_ptr);

@@ -152,3 +152,27 @@ def test_staged_agrees_with_plain(ctx):
 def test_staged_rejects_nearest(ctx, vol24):
     with pytest.raises(wrt.WrtError):
         ctx.radon_grid(vol24, 4, 4, 4, sampler=O.NEAREST, kernel=wrt.KERNEL_STAGED)
+
+
+def test_every_staged_tile_configuration_matches_oracle(ctx):
+    vol = ellipsoid_phantom(40, 8, 515)
+    ref = O.radon_forward(vol, 10, 6, 15, sampler=O.TRILINEAR, half_extent=40)
+    try:
+        for k, shape in enumerate(wrt.plane_kernel_configs()):
+            wrt.set_plane_kernel_config(ctx, k)
+            got = ctx.radon_grid(vol, 10, 6, 15, sampler=O.TRILINEAR, half_extent=40,
+                                 kernel=wrt.KERNEL_STAGED)
+            assert rel_l2(got, ref) < TOL_L2, shape
+    finally:
+        wrt.set_plane_kernel_config(ctx, -1)
+
+
+def test_autotuner_picks_a_configuration(ctx):
+    vol = wrt.Volume(ctx, 32)
+    vol.upload(ellipsoid_phantom(32, 6, 9))
+    grid = wrt.Grid(ctx, 12, 6, 16)
+    out = wrt.DeviceBuffer(ctx, grid.nplanes * 8)
+    best, ms = wrt.tune_plane_kernel(ctx, vol, grid, out.ptr, half_extent=32)
+    assert 0 <= best < len(wrt.plane_kernel_configs()) and ms > 0
+    wrt.set_plane_kernel_config(ctx, -1)
+    out.close(); grid.close(); vol.close()

@@ -100,6 +100,11 @@ def lib() -> C.CDLL:
         L.wrt_host_free_pinned.argtypes = [_vp, _vp]
         L.wrt_copy_to_device.argtypes = [_vp, _vp, _vp, _sz]
         L.wrt_copy_to_host.argtypes = [_vp, _vp, _vp, _sz]
+        L.wrt_tune_plane_kernel.argtypes = [_vp, _vp, _vp, C.POINTER(PlaneOpts), _vp,
+                                            C.POINTER(_i), C.POINTER(C.c_float)]
+        L.wrt_plane_kernel_config_describe.argtypes = [_i, C.POINTER(_i), C.POINTER(_i),
+                                                       C.POINTER(_i)]
+        L.wrt_ctx_set_plane_kernel_config.argtypes = [_vp, _i]
         _lib = L
     return _lib
 
@@ -372,3 +377,28 @@ def radon_forward_device(ctx: Context, vol: Volume, grid: Grid, dev_out: int, sa
     o = plane_opts(sampler, half_extent, kernel)
     ctx.check(lib().wrt_radon_forward_device(ctx.handle, vol.handle, grid.handle, C.byref(o),
                                              _vp(dev_out)), "radon_forward_device")
+
+
+def plane_kernel_configs():
+    """Tile shapes of the staged plane kernel: list of (threads, rows per
+    group, shifts per lane)."""
+    out = []
+    for k in range(lib().wrt_plane_kernel_config_count()):
+        t, g, s = _i(), _i(), _i()
+        lib().wrt_plane_kernel_config_describe(k, C.byref(t), C.byref(g), C.byref(s))
+        out.append((t.value, g.value, s.value))
+    return out
+
+
+def set_plane_kernel_config(ctx: Context, index: int):
+    ctx.check(lib().wrt_ctx_set_plane_kernel_config(ctx.handle, int(index)), "set config")
+
+
+def tune_plane_kernel(ctx: Context, vol: Volume, grid: Grid, dev_out: int, sampler=TRILINEAR,
+                      half_extent=0):
+    """Run the autotuner on this request; returns (best index, ms per launch)."""
+    o = plane_opts(sampler, half_extent, KERNEL_STAGED)
+    best, ms = _i(), C.c_float()
+    ctx.check(lib().wrt_tune_plane_kernel(ctx.handle, vol.handle, grid.handle, C.byref(o),
+                                          _vp(dev_out), C.byref(best), C.byref(ms)), "tune")
+    return best.value, float(ms.value)

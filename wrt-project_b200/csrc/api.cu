@@ -568,6 +568,63 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const wrt_gri
   return plane_forward_plain(ctx, job);
 }
 
+int wrt_plane_kernel_config_count(void) { return kNumStagedConfigs; }
+
+int wrt_plane_kernel_config_describe(int index, int *threads, int *rows_per_group,
+                                     int *shifts_per_lane) {
+  if (index < 0 || index >= kNumStagedConfigs) return WRT_ERR_INVALID_ARGUMENT;
+  if (threads) *threads = kStagedConfigs[index].threads;
+  if (rows_per_group) *rows_per_group = kStagedConfigs[index].group;
+  if (shifts_per_lane) *shifts_per_lane = kStagedConfigs[index].shifts_per_lane;
+  return WRT_OK;
+}
+
+int wrt_ctx_set_plane_kernel_config(wrt_ctx *ctx, int index) {
+  if (!ctx || index < -1 || index >= kNumStagedConfigs) return WRT_ERR_INVALID_ARGUMENT;
+  ctx->staged_config = index;
+  return WRT_OK;
+}
+
+int wrt_tune_plane_kernel(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *grid,
+                          const wrt_plane_opts *opts, double *dev_out, int *best,
+                          float *best_ms) {
+  if (!ctx || !vol || !grid || !dev_out) return WRT_ERR_INVALID_ARGUMENT;
+  wrt_plane_opts o = {};
+  if (opts) o = *opts;
+  o.kernel = WRT_KERNEL_STAGED;
+  cudaEvent_t a, b;
+  if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
+    return fail(ctx, WRT_ERR_CUDA, "tuner events");
+  int st = WRT_OK, best_i = -1;
+  float best_t = 0.0f;
+  for (int c = 0; c < kNumStagedConfigs && !st; ++c) {
+    ctx->staged_config = c;
+    st = wrt_radon_forward_device(ctx, vol, grid, &o, dev_out);  // warm-up
+    float tmin = 0.0f;
+    for (int rep = 0; rep < 3 && !st; ++rep) {
+      cudaEventRecord(a, ctx->stream);
+      st = wrt_radon_forward_device(ctx, vol, grid, &o, dev_out);
+      cudaEventRecord(b, ctx->stream);
+      if (!st && cudaEventSynchronize(b) != cudaSuccess) st = fail(ctx, WRT_ERR_CUDA, "tuner sync");
+      float ms = 0.0f;
+      if (!st) cudaEventElapsedTime(&ms, a, b);
+      if (rep == 0 || ms < tmin) tmin = ms;
+    }
+    if (!st && (best_i < 0 || tmin < best_t)) {
+      best_i = c;
+      best_t = tmin;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  ctx->staged_config = st ? -1 : best_i;
+  if (!st) {
+    if (best) *best = best_i;
+    if (best_ms) *best_ms = best_t;
+  }
+  return st;
+}
+
 // -------------------------------------------------------- drop-in, host I/O
 int wrt_radon_grid(wrt_ctx *ctx, const double *volume, int n, int nphi, int ntheta, int nshift,
                    const wrt_plane_opts *opts, double *out) {

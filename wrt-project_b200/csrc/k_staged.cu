@@ -39,10 +39,11 @@
 
 namespace {
 
-constexpr int kThreads = 768;
-constexpr int kWarps = kThreads / 32;
-constexpr int kShiftsPerLane = 4;  // a warp enumerates 128 shifts at a time
 constexpr unsigned kFull = 0xffffffffu;
+// x + 1.5 * 2^23 rounds x to an integer held in the low mantissa bits
+// (|x| < 2^22); subtracting the constant's bit pattern recovers it.
+constexpr float kMagic = 12582912.0f;
+constexpr int kMagicBits = 0x4B400000;
 
 __device__ __forceinline__ float row_w(float s, float nz, float a1z, float di, float h) {
   return (fmaf(di, a1z, s * nz) + 1.0f) * h;
@@ -105,10 +106,15 @@ __device__ __noinline__ double exact_sample(const wrt::StagedReq &R, int d, int 
   return wrtd::exact_trilinear(R.vol, R.n, px, py, pz);
 }
 
+// kThreads: CTA size (one CTA per SM); kGroup: rows a warp walks together
+// (32/kGroup lanes per row); kShiftsPerLane: shifts a lane enumerates per
+// pass (a pass covers 32*kShiftsPerLane shifts).
+template <int kThreads, int kGroup, int kShiftsPerLane>
 __global__ void __launch_bounds__(kThreads, 1)
     plane_staged_kernel(const wrt::StagedReq *__restrict__ reqs,
                         const wrt::StagedItem *__restrict__ items, int nitems,
                         int *__restrict__ next_item, unsigned long long *__restrict__ counter) {
+  constexpr int kLanesPerRow = 32 / kGroup;
   extern __shared__ float4 quads[];
   __shared__ int s_item, s_dir;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -239,26 +245,45 @@ __global__ void __launch_bounds__(kThreads, 1)
               }
             }
           }
-          // ---- walk the row
-          double row_acc = 0.0;
-          int j = jlo;
-          while (__any_sync(kFull, j <= jhi)) {
+          // ---- walk the rows in groups of kGroup, kLanesPerRow lanes per row,
+          // consecutive samples on consecutive lanes of a row
+          const int nrows = min(32, total - r0);
+          for (int g0 = 0; g0 < nrows; g0 += kGroup) {
+            const int rr = g0 + lane / kLanesPerRow, pos = lane % kLanesPerRow;
+            const bool rvalid = rr < nrows;
+            const int src = rvalid ? rr : 0;
+            const int k_is = __shfl_sync(kFull, is, src), k_i = __shfl_sync(kFull, i, src);
+            const int k_jlo = __shfl_sync(kFull, jlo, src);
+            const int jhi_src = __shfl_sync(kFull, jhi, src);
+            const int k_jhi = rvalid ? jhi_src : k_jlo - 1;
+            const float k_ubm = __shfl_sync(kFull, ub, src) - 0.5f;  // q - 1/2 at j = 0
+            const float k_vbm = __shfl_sync(kFull, vb, src) - 0.5f;
+            const float k_tz = __shfl_sync(kFull, tz, src);
+            const bool k_zx = __shfl_sync(kFull, (int)zexact, src) != 0;
+            const int len = max(0, k_jhi - k_jlo + 1);
+            const int trips = (int)__reduce_max_sync(kFull, (unsigned)((len + kLanesPerRow - 1) / kLanesPerRow));
+            const float jhif = (float)k_jhi;
+            float jf = (float)(k_jlo + pos);
             float part = 0.0f;
-#pragma unroll 4
-            for (int t = 0; t < 32; ++t, ++j) {
-              if (j <= jhi) {
-                const float jf = (float)j;
-                const float qx = fmaf(jf, du, ub), qy = fmaf(jf, dv, vb);
-                const float fx = floorf(qx), fy = floorf(qy);
-                const float tx = qx - fx, ty = qy - fy;
-                const bool band = zexact | (fmaxf(fabsf(tx - 0.5f), fabsf(ty - 0.5f)) > halfband);
-                const int ix = (int)fx, iy = (int)fy - y0;
+            double xacc = 0.0;  // guard-band samples, FP64
+            for (int t = 0; t < trips; ++t, jf += (float)kLanesPerRow) {
+              if (jf <= jhif) {
+                // cell = round-to-nearest(q - 1/2) via the 1.5 * 2^23 shift (no
+                // float-to-int conversion instructions); d = frac(q) - 1/2
+                const float qx = fmaf(jf, du, k_ubm), qy = fmaf(jf, dv, k_vbm);
+                const float sx = qx + kMagic, sy = qy + kMagic;
+                const float fx = sx - kMagic, fy = sy - kMagic;
+                const float dx = qx - fx, dy = qy - fy;
+                const int ix = __float_as_int(sx) - kMagicBits;
+                const int iy = __float_as_int(sy) - kMagicBits - y0;
+                const bool band = k_zx | (fmaxf(fabsf(dx), fabsf(dy)) > halfband);
                 if (!band) {
                   if ((unsigned)ix < (unsigned)W && (unsigned)iy < (unsigned)H) {
+                    const float tx = dx + 0.5f, ty = dy + 0.5f;
                     const float4 *q = quads + iy * qp + ix;
                     const float4 a = q[0], b = q[qp];
-                    const float va = fmaf(tx, fmaf(tz, a.w, a.z), fmaf(tz, a.y, a.x));
-                    const float vb2 = fmaf(tx, fmaf(tz, b.w, b.z), fmaf(tz, b.y, b.x));
+                    const float va = fmaf(tx, fmaf(k_tz, a.w, a.z), fmaf(k_tz, a.y, a.x));
+                    const float vb2 = fmaf(tx, fmaf(k_tz, b.w, b.z), fmaf(k_tz, b.y, b.x));
                     part += fmaf(ty, vb2 - va, va);
                     ++evaluated;
                   }
@@ -266,28 +291,29 @@ __global__ void __launch_bounds__(kThreads, 1)
                   // a guard-band sample belongs to the tile of its FP32 cell row,
                   // clamped to the grid (samples within the band outside a face
                   // are evaluated, and cut off, by the FP64 reference arithmetic)
-                  const int cy = min(max((int)fy, 0), W - 1) - y0;
+                  const int cy = min(max(iy + y0, 0), W - 1) - y0;
                   if ((unsigned)cy < (unsigned)H) {
-                    row_acc += exact_sample(R, d, is, i, j);
+                    xacc += exact_sample(R, d, k_is, k_i, (int)jf);
                     ++evaluated;
                   }
                 }
               }
             }
-            row_acc += (double)part;
-          }
-          // ---- fixed-point accumulation, segmented by plane over the warp
-          long long v = valid ? __double2ll_rn(row_acc * R.scale) : 0LL;
-          const int key = valid ? is : -1;
+            // ---- fixed-point accumulation, segmented by plane over the warp
+            // (rows are ordered by shift, so lanes of one plane are contiguous)
+            const double row_acc = xacc + (double)part;
+            long long v = rvalid ? __double2ll_rn(row_acc * R.scale) : 0LL;
+            const int key = rvalid ? k_is : -1;
 #pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const long long t = __shfl_up_sync(kFull, v, o);
-            const int k2 = __shfl_up_sync(kFull, key, o);
-            if (lane >= o && k2 == key) v += t;
+            for (int o = 1; o < 32; o <<= 1) {
+              const long long tv = __shfl_up_sync(kFull, v, o);
+              const int k2 = __shfl_up_sync(kFull, key, o);
+              if (lane >= o && k2 == key) v += tv;
+            }
+            const int knext = __shfl_down_sync(kFull, key, 1);
+            if (rvalid && (lane == 31 || knext != key) && v != 0)
+              atomicAdd(R.acc + (size_t)k_is * R.ndir + d, (unsigned long long)v);
           }
-          const int knext = __shfl_down_sync(kFull, key, 1);
-          if (valid && (lane == 31 || knext != key) && v != 0)
-            atomicAdd(R.acc + (size_t)is * R.ndir + d, (unsigned long long)v);
         }
       }
     }
@@ -326,17 +352,41 @@ int staged_smem_bytes(int n, int *tile_h, int *qpitch) {
   return (th + 1) * qp * 16;
 }
 
-int plane_staged_launch(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items,
-                        int nitems, int max_smem, int *d_next) {
-  cudaError_t e = cudaFuncSetAttribute(plane_staged_kernel,
+namespace {
+template <int T, int G, int K>
+int launch_cfg(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items, int nitems,
+               int max_smem, int *d_next) {
+  cudaError_t e = cudaFuncSetAttribute(plane_staged_kernel<T, G, K>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged kernel smem attribute");
   e = cudaMemsetAsync(d_next, 0, sizeof(int), ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged counter reset");
-  plane_staged_kernel<<<ctx->sm_count, kThreads, max_smem, ctx->stream>>>(d_reqs, d_items, nitems,
-                                                                          d_next, ctx->d_counter);
+  plane_staged_kernel<T, G, K><<<ctx->sm_count, T, max_smem, ctx->stream>>>(
+      d_reqs, d_items, nitems, d_next, ctx->d_counter);
   ctx->launches++;
   return check_launch(ctx, "plane_staged_kernel");
+}
+}  // namespace
+
+// The tile shapes the autotuner chooses among: (CTA threads, rows per warp
+// group, shifts per lane per enumeration pass).
+const StagedConfig kStagedConfigs[] = {
+    {512, 4, 4}, {512, 8, 4}, {512, 2, 4}, {640, 4, 2}, {768, 4, 2}, {768, 8, 2},
+};
+const int kNumStagedConfigs = sizeof(kStagedConfigs) / sizeof(kStagedConfigs[0]);
+
+int plane_staged_launch(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items,
+                        int nitems, int max_smem, int *d_next) {
+  const int c = (ctx->staged_config >= 0 && ctx->staged_config < kNumStagedConfigs)
+                    ? ctx->staged_config : 0;
+  switch (c) {
+    case 0: return launch_cfg<512, 4, 4>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
+    case 1: return launch_cfg<512, 8, 4>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
+    case 2: return launch_cfg<512, 2, 4>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
+    case 3: return launch_cfg<640, 4, 2>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
+    case 4: return launch_cfg<768, 4, 2>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
+    default: return launch_cfg<768, 8, 2>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
+  }
 }
 
 int plane_finalize(wrt_ctx *ctx, double *out, long long count, double factor) {
@@ -418,7 +468,7 @@ int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir
       c->lists.clear();
     }
     std::vector<StagedItem> items;
-    const int chunk = 128;  // directions per item
+    const int chunk = 512;  // directions per item
     staged_items(0, n, tile_h, crop_r2, ndir, chunk, items);
     ItemList l;
     l.count = (int)items.size();

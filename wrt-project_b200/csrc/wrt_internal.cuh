@@ -52,6 +52,7 @@ struct wrt_ctx {
   size_t staged_req_bytes = 0;
   int *staged_next = nullptr;
   void *staged_cache = nullptr;
+  int staged_config = -1;  // tile configuration (-1: default), set by the autotuner
 };
 
 namespace wrt {
@@ -114,6 +115,11 @@ struct StagedReq {
 struct StagedItem {
   int req, layer, tile, dir0, ndir;
 };
+struct StagedConfig {
+  int threads, group, shifts_per_lane;
+};
+extern const StagedConfig kStagedConfigs[];
+extern const int kNumStagedConfigs;
 int staged_smem_bytes(int n, int *tile_h, int *qpitch);
 int plane_staged_launch(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items,
                         int nitems, int max_smem, int *d_next);
