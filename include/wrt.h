@@ -127,6 +127,24 @@ int wrt_radon_reduction(wrt_ctx *ctx, const double *rays, int ngrid, int nshift_
 int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
                         int nshift, int ngrid, double *out);
 
+/* The backprojection of wrt_radon3d_adjoint without allocating any device
+ * memory.  No counterpart in the reference.  For callers that cannot call
+ * cudaMalloc: programs that give all device memory to their own allocator or
+ * reserve it up front, and latency-critical pipelines that forbid allocation
+ * after start-up (cudaMalloc/cudaFree synchronise the device).  d_radon
+ * (nshift*nphi*ntheta doubles, order [is][iphi][itheta]) and d_out (ngrid^3
+ * doubles, order [iz][ix][iy]) are device buffers owned by the caller; the
+ * working memory is one fixed ~6.3 MB array inside the library, held by every
+ * GPU that loads the library until the process exits.  Limits: nphi*ntheta
+ * <= 16384, ntheta <= 1024, 3 <= nshift <= 2048, nphi*ntheta*nshift <=
+ * 262144; larger sizes return WRT_ERR_INVALID_ARGUMENT with a message.  The
+ * first call on a device looks up the array's device address (make that first
+ * call before any stream capture).  Asynchronous on the context's stream.
+ * Every call shares the array: calls whose GPU work overlaps (other streams,
+ * other contexts on the same device) race and must be ordered by the caller. */
+int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta,
+                               int nshift, int ngrid, double *d_out);
+
 /* Exact transpose of wrt_radon_grid with the same options: out_volume (n^3,
  * v[ix][iy][iz] order) = R^T g.  No counterpart in the reference; it makes
  * the adjoint identity <R f, g> = <f, R^T g> testable. */

@@ -133,6 +133,14 @@ int sphere_grid(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *phi, dou
   return WRT_OK;
 }
 
+// Gauss-Legendre nodes into caller-provided device memory, on a given stream
+// (used by the allocation-free adjoint entry point).
+int launch_gl_nodes(cudaStream_t stream, int n, double *d_x, double *d_w) {
+  const int threads = 128, blocks = (n / 2 + 1 + threads - 1) / threads;
+  gl_nodes_kernel<<<blocks, threads, 0, stream>>>(n, d_x, d_w);
+  return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
+}
+
 // radon_grid/src/integral.c:10-36: normal = omega(phi, theta),
 // v1 = omega(phi, theta + pi/2), v2 = normal x v1.
 void plane_directions(int nphi, const double *phi, int ntheta, const double *theta,

@@ -195,6 +195,26 @@ int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long l
 
 namespace wrt {
 
+// Launchers over caller-provided device memory (used by the allocation-free
+// adjoint entry point): spline preparation of the nphi*ntheta lines of a
+// Radon data set ([nshift][nphi][ntheta]) and the adjoint proper.
+int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
+                         const double *d_cp, const double *d_den, double *d_scratch,
+                         float4 *d_lines) {
+  spline_prep_kernel<<<(ndir + 127) / 128, 128, 0, stream>>>(
+      d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, 2.0 / (nshift - 1), d_cp, d_den,
+      d_scratch, d_lines);
+  return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
+}
+
+int launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int ntheta, int nshift,
+                   const float4 *d_dirw, int n, double *d_out) {
+  const long long total = (long long)n * n * n;
+  adjoint_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_lines, ndir, ntheta,
+                                                                        nshift, d_dirw, n, d_out);
+  return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
+}
+
 int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_ray, int nphi,
                       const double *d_shift, int nshift, const double *d_cs, int ntheta,
                       double *d_out) {
