@@ -255,6 +255,82 @@ def traffic_from_profiles():
     return None
 
 
+def served_stream(wrt, srv, pin_vol, pin_outs, steps):
+    """K requests of the workload through the serving loop, each with its FP32
+    volume in pinned host memory and its FP64 result copied back to pinned
+    host memory.  Returns (wall seconds, infos)."""
+    t0 = time.perf_counter()
+    ids = [srv.submit_forward(pin_vol, NPHI, NTHETA, NSHIFT, pin_outs[k % len(pin_outs)],
+                              half_extent=HALF_EXTENT, tag=k) for k in range(steps)]
+    infos = [srv.wait(i) for i in ids]
+    return time.perf_counter() - t0, infos
+
+
+def serving_mix(wrt, dev, count, seed, budget):
+    """A Poisson stream of mixed requests (the serving configuration, scaled to
+    `count` requests): edge 64/96/128/192/256 w.p. .30/.25/.20/.15/.10,
+    forward (80 %) or adjoint (20 %), sphere grids 32x64 .. 96x192 (latitudes
+    x longitudes), 128-384 shifts, FP32 volumes of seeded ellipsoids, seeded
+    Gaussian Radon data for the adjoints.  Arrival rate: ~90 % of the measured
+    service rate of a first batch."""
+    from wrt_b200.phantom import ellipsoid_phantom
+
+    rng = np.random.default_rng(seed)
+    edges = rng.choice([64, 96, 128, 192, 256], size=count, p=[0.30, 0.25, 0.20, 0.15, 0.10])
+    vol_cache = {}
+    reqs = []
+    for k in range(count):
+        n = int(edges[k])
+        nth = int(rng.integers(32, 97))
+        ns = int(rng.integers(128, 385))
+        if rng.random() < 0.8:
+            if n not in vol_cache:
+                vol_cache[n] = ellipsoid_phantom(n, 12, seed + n).astype(np.float32)
+            reqs.append(("fwd", n, nth, ns))
+        else:
+            reqs.append(("adj", n, nth, ns))
+    adj_data = {}
+    with wrt.Server(dev, budget_bytes=budget, max_batch=16, max_inflight=2) as srv:
+        def submit(r):
+            op, n, nth, ns = r
+            if op == "fwd":
+                out = np.empty((ns, 2 * nth, nth))
+                return srv.submit_forward(vol_cache[n], 2 * nth, nth, ns, out, half_extent=n), out
+            key = (nth, ns)
+            if key not in adj_data:
+                adj_data[key] = rng.standard_normal((ns, 2 * nth, nth))
+            out = np.empty((n, n, n))
+            return srv.submit_adjoint(adj_data[key], n, out), out
+        # service-rate estimate from the first few requests run back to back
+        t0 = time.perf_counter()
+        warm = [submit(r) for r in reqs[:8]]
+        for rid, _ in warm:
+            srv.wait(rid)
+        rate = 8 / (time.perf_counter() - t0) * 0.9
+        gaps = rng.exponential(1.0 / rate, size=count)
+        t_start = time.perf_counter()
+        pending, t_next = [], t_start
+        for k, r in enumerate(reqs):
+            t_next += gaps[k]
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            pending.append((r, submit(r)))
+        infos = [(r, srv.wait(rid)) for r, (rid, _) in pending]
+        wall = time.perf_counter() - t_start
+        st = srv.stats()
+    lat = np.array([i.done_ms - i.submit_ms for _, i in infos])
+    planes = sum(r[3] * 2 * r[2] * r[2] for r, _ in infos if r[0] == "fwd")
+    return {"requests": count, "forward": sum(r[0] == "fwd" for r in reqs),
+            "arrival_rate_per_s": rate, "wall_s": wall,
+            "requests_per_s": count / wall, "plane_integrals_per_s": planes / wall,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99))},
+            "launches": int(st.launches), "hbm_peak_bytes": int(st.bytes_peak),
+            "budget_bytes": int(st.budget),
+            "mean_batch": float(np.mean([i.batch_size for _, i in infos]))}
+
+
 def run_ours(args, dist):
     wrt = load_package()
     from wrt_b200.phantom import ellipsoid_phantom
@@ -263,21 +339,28 @@ def run_ours(args, dist):
     ctx = wrt.Context(dev)
     phantom = ellipsoid_phantom(N, ELLIPSOIDS, SEED)
     vol = wrt.Volume(ctx, N)
-    vol.upload(phantom)
+    vol.upload(phantom.astype(np.float32))
     grid = wrt.Grid(ctx, NPHI, NTHETA, NSHIFT)
     nplanes = grid.nplanes
     out = wrt.DeviceBuffer(ctx, nplanes * 8)
     kernel = {"plain": wrt.KERNEL_PLAIN, "staged": wrt.KERNEL_STAGED, "auto": wrt.KERNEL_AUTO}[args.kernel]
 
     def step(k=kernel):
-        wrt.radon_forward_device(ctx, vol, grid, out.ptr, sampler=wrt.TRILINEAR,
-                                 half_extent=HALF_EXTENT, kernel=k)
+        if k == wrt.KERNEL_PLAIN:
+            wrt.radon_forward_device(ctx, vol, grid, out.ptr, sampler=wrt.TRILINEAR,
+                                     half_extent=HALF_EXTENT, kernel=k)
+        else:  # the batched persistent kernel through its captured graph
+            wrt.radon_forward_batch(ctx, [(vol, grid, out.ptr, HALF_EXTENT)])
 
     # the autotuner picks the staged kernel's tile shape on this request
     tile = None
     if kernel != wrt.KERNEL_PLAIN:
-        best, best_ms = wrt.tune_plane_kernel(ctx, vol, grid, out.ptr, sampler=wrt.TRILINEAR,
-                                              half_extent=HALF_EXTENT)
+        if args.tile is not None:
+            best, best_ms = args.tile, None
+            wrt.set_plane_kernel_config(ctx, best)
+        else:
+            best, best_ms = wrt.tune_plane_kernel(ctx, vol, grid, out.ptr, sampler=wrt.TRILINEAR,
+                                                  half_extent=HALF_EXTENT)
         t, g, s = wrt.plane_kernel_configs()[best]
         tile = {"threads": t, "rows_per_warp_group": g, "shifts_per_lane": s,
                 "tuner_ms": best_ms}
@@ -310,6 +393,7 @@ def run_ours(args, dist):
     total_ms = dist.max(sum(times))
     ms_per_step = total_ms / args.steps
     value = nplanes * args.steps * dist.world / (total_ms * 1e-3)
+    result_dev = out.download(np.empty((NSHIFT, NPHI, NTHETA)))
 
     # plain kernel alongside (the one-request-per-launch baseline)
     plain = None
@@ -321,28 +405,28 @@ def run_ours(args, dist):
             ctx.timer_start()
             step(wrt.KERNEL_PLAIN)
             pt.append(ctx.timer_stop())
+        plain_res = out.download(np.empty((NSHIFT, NPHI, NTHETA)))
         plain = {"value": nplanes / (statistics.mean(pt) * 1e-3), "unit": UNIT,
-                 "ms_per_step": statistics.mean(pt)}
+                 "ms_per_step": statistics.mean(pt),
+                 "rel_l2_vs_staged": float(np.linalg.norm(plain_res - result_dev) /
+                                           np.linalg.norm(result_dev))}
 
-    # end to end through the public API: FP64 volume in from pinned host
-    # memory, resident grid, FP64 results back to pinned host memory
-    pin_in = wrt.PinnedArray(ctx, (N, N, N), np.float64)
-    pin_in.array[...] = phantom
-    pin_out = wrt.PinnedArray(ctx, (NSHIFT, NPHI, NTHETA), np.float64)
-    for _ in range(2):
-        vol.upload(pin_in.array)
-        step()
-        out.download(pin_out.array)
+    # end to end through the serving loop (the public API a caller uses): each
+    # step is one request of the workload, its FP32 volume copied in from pinned
+    # host memory and its FP64 plane integrals copied back to pinned host memory
+    pin_vol = wrt.PinnedArray(ctx, (N, N, N), np.float32)
+    pin_vol.array[...] = phantom
+    pin_outs = [wrt.PinnedArray(ctx, (NSHIFT, NPHI, NTHETA), np.float64) for _ in range(4)]
+    srv = wrt.Server(dev, budget_bytes=4 << 30, max_batch=8, max_inflight=2)
+    served_stream(wrt, srv, pin_vol.array, [p.array for p in pin_outs], 3)  # warm-up
     dist.barrier()
-    e2e_times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        vol.upload(pin_in.array)
-        step()
-        out.download(pin_out.array)
-        e2e_times.append(time.perf_counter() - t0)
-    e2e_total = dist.max(sum(e2e_times))
-    e2e_value = nplanes * args.steps * dist.world / e2e_total
+    wall, infos = served_stream(wrt, srv, pin_vol.array, [p.array for p in pin_outs], args.steps)
+    served_res = np.array(pin_outs[(args.steps - 1) % len(pin_outs)].array)
+    srv.close()
+    wall = dist.max(wall)
+    e2e_value = nplanes * args.steps * dist.world / wall
+    lat = np.array([i.done_ms - i.submit_ms for i in infos])
+    served_equal = bool(np.array_equal(served_res, result_dev))
 
     # roofline of the plane kernel: 32 B of staged voxel reads per sample
     # against the measured shared-memory bandwidth of this device
@@ -364,11 +448,11 @@ def run_ours(args, dist):
                                "lattice step 1/n on [-n,n)^2",
                    "n": N, "sphere_grid": [NTHETA, NPHI], "shifts": NSHIFT,
                    "planes_per_step": nplanes, "kernel": args.kernel, "tile": tile,
+                   "path": "batched persistent kernel, graph launch (wrt_radon_forward_batch)",
                    "l2": "flushed before every timed step (2x L2 memset)",
                    "parallelism": f"replicas x{dist.world}"},
         "samples_per_step": samples,
         "samples_per_s": samples * args.steps * dist.world / (total_ms * 1e-3),
-        "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
         "gpu_launches": launches,
         "roofline": {"bound": "l1tex", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic_from_profiles(),
@@ -377,18 +461,27 @@ def run_ours(args, dist):
                      "hbm": {"achieved": hbm_bytes / per_launch_s / 1e9, "peak": hbm_peak,
                              "unit": "GB/s", "frac": hbm_bytes / per_launch_s / 1e9 / hbm_peak,
                              "note": "compulsory bytes only; the volume is re-read from L2"}},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N ** 3 * 8,
-                "d2h_bytes_per_step": nplanes * 8},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N ** 3 * 4,
+                "d2h_bytes_per_step": nplanes * 8,
+                "path": "wrt_server: one request per step, pinned FP32 volume in, pinned FP64 "
+                        "results out, 2 launches in flight",
+                "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                               "p99": float(np.percentile(lat, 99))},
+                "result_bitwise_equal_to_kernel_path": served_equal},
         "clocks": clk,
     }
     if plain:
         result["plain"] = plain
+        result["served_over_plain"] = e2e_value / plain["value"]
+    if dist.rank == 0 and dist.world == 1 and not args.no_serving_mix:
+        result["serving"] = serving_mix(wrt, dev, args.mix_requests, 4000, 60 << 30)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(phantom)
     if dist.rank == 0:
         print(json.dumps(result))
-    pin_in.close()
-    pin_out.close()
+    pin_vol.close()
+    for p in pin_outs:
+        p.close()
     out.close()
     vol.close()
     grid.close()
@@ -404,6 +497,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--kernel", choices=["auto", "plain", "staged"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving-mix", action="store_true")
+    ap.add_argument("--mix-requests", type=int, default=96,
+                    help="requests in the mixed serving stream")
+    ap.add_argument("--tile", type=int, default=None,
+                    help="use this tile configuration of the staged kernel instead of tuning")
     ap.add_argument("--grid", default=None,
                     help="NPHI,NTHETA,NSHIFT: a smaller sphere grid (profiling captures only)")
     args = ap.parse_args()

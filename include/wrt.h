@@ -21,8 +21,8 @@
  *   adjoint A[iz][ix][iy]          (backprojection/C/src/radon3d_ajoint.c:240-254)
  *
  * Threading: a wrt_ctx is used by one host thread at a time.  A wrt_server
- * owns its own dispatcher thread; wrt_server_submit/poll may be called from
- * any thread.
+ * owns its own dispatcher and completion threads; wrt_server_submit/wait may
+ * be called from any thread.
  */
 #ifndef WRT_H
 #define WRT_H
@@ -171,6 +171,29 @@ int wrt_grid_destroy(wrt_grid *grid);
 int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *grid,
                              const wrt_plane_opts *opts, double *dev_out);
 
+/* One request of a batch: the plane integrals of a resident volume on a
+ * resident sphere grid (trilinear sampler, lattice [-L, L)^2 with step 1/n,
+ * L = half_extent or 2n when 0) into dev_out, nshift*nphi*ntheta doubles in
+ * the order of wrt_radon_grid. */
+typedef struct wrt_forward_req {
+  const wrt_volume *volume;
+  const wrt_grid *grid;
+  int half_extent;
+  int reserved;
+  double *dev_out;
+} wrt_forward_req;
+
+/* Up to 256 forward requests (volumes of any edge length, each with its own
+ * sphere grid) in ONE launch of the persistent staged kernel: the work items
+ * of all requests are ordered by cost and shared by all SMs.  The launch
+ * sequence (table upload, output reset, request set-up, plane kernel,
+ * finalize) is a CUDA graph captured once per context and replayed with a new
+ * request table.  Asynchronous on the context's stream.  Each result is
+ * bitwise identical to what wrt_radon_forward_device gives for the same
+ * request alone.  Batch transforms of the reference's loop nest
+ * radon_grid/src/radon_grid.c:229-264, one per request. */
+int wrt_radon_forward_batch(wrt_ctx *ctx, const wrt_forward_req *reqs, int nreq);
+
 /* The context's CUDA stream (cudaStream_t), for callers that order their own
  * work against the library's. */
 void *wrt_ctx_stream(wrt_ctx *ctx);
@@ -198,6 +221,74 @@ int wrt_host_free_pinned(wrt_ctx *ctx, void *host_ptr);
 /* Copies ordered on the context's stream; the device-to-host copy waits. */
 int wrt_copy_to_device(wrt_ctx *ctx, void *dev_dst, const void *host_src, size_t bytes);
 int wrt_copy_to_host(wrt_ctx *ctx, void *host_dst, const void *dev_src, size_t bytes);
+
+/* ---------------------------------------------------------------- serving */
+/* A request loop for many callers: a wrt_server keeps its device context, the
+ * sphere-grid tables of the shapes it has seen and one arena of device memory
+ * (its HBM budget, reserved at creation) resident, admits queued requests in
+ * arrival order as launch slots and memory free up, and runs each admitted
+ * set as ONE batch launch (the graph of wrt_radon_forward_batch, plus the
+ * backprojections).  With max_inflight >= 2 a batch is formed and queued
+ * while the previous one runs (continuous batching).  A request's result is
+ * bitwise the same whatever batch it runs in.  No counterpart in the
+ * reference, whose programs answer one request per process run. */
+typedef struct wrt_server wrt_server;
+
+typedef enum wrt_op {
+  WRT_OP_FORWARD = 0, /* plane integrals, trilinear sampler (radon_grid/src/integral.c:26) */
+  WRT_OP_ADJOINT = 1  /* backprojection (radon_inversion/backprojection/C/src/integral.c:6) */
+} wrt_op;
+
+typedef struct wrt_request {
+  int op;              /* wrt_op */
+  int ngrid;           /* n: edge of the input (forward) or output (adjoint) volume */
+  int nphi, ntheta, nshift;
+  int half_extent;     /* forward: lattice [-L, L)^2 with step 1/n; 0 means L = 2n */
+  const float *volume; /* forward input: n^3 FP32 values, v[ix][iy][iz] */
+  const double *radon; /* adjoint input: nshift*nphi*ntheta values, [is][iphi][itheta] */
+  double *out;         /* result: forward [is][iphi][itheta]; adjoint [iz][ix][iy] */
+  uint64_t tag;        /* the caller's, returned in wrt_request_info */
+} wrt_request;
+
+typedef struct wrt_request_info {
+  int status;          /* wrt_status of the request */
+  int batch_size;      /* requests in the launch that ran it */
+  uint64_t tag;
+  double submit_ms, start_ms, done_ms; /* server clock: submission, launch, result in out */
+} wrt_request_info;
+
+typedef struct wrt_server_opts {
+  int device;          /* CUDA ordinal */
+  int max_batch;       /* requests per launch (0: 64; at most 256 forward + 256 adjoint) */
+  int max_inflight;    /* launches on the device at once (0: 2; at most 8) */
+  int queue_capacity;  /* requests waiting for admission (0: 65536) */
+  size_t hbm_budget;   /* device memory for request state and grid tables
+                          (0: 60 GiB or 3/4 of the free memory, whichever is less) */
+  int reserved[8];
+} wrt_server_opts;
+
+typedef struct wrt_server_stats {
+  uint64_t submitted, completed, failed, launches;
+  size_t budget, bytes_in_use, bytes_peak;
+  size_t queued, in_flight, grid_shapes;
+} wrt_server_stats;
+
+/* opts may be NULL (defaults). */
+int wrt_server_create(const wrt_server_opts *opts, wrt_server **out);
+/* Queues a request (copied; the buffers it points to must stay valid until
+ * wrt_server_wait returns for it).  Host buffers in pinned memory
+ * (wrt_host_alloc_pinned) are copied asynchronously; pageable ones are copied
+ * synchronously by the server's threads.  Returns WRT_ERR_QUEUE_FULL when the
+ * queue is full, WRT_ERR_BUDGET when the request can never fit the budget. */
+int wrt_server_submit(wrt_server *srv, const wrt_request *req, uint64_t *id);
+/* Waits up to timeout_ms (< 0: without limit, 0: poll) for a request; on
+ * completion fills info (may be NULL), forgets the id and returns the
+ * request's status; WRT_ERR_TIMEOUT if it is still running. */
+int wrt_server_wait(wrt_server *srv, uint64_t id, int timeout_ms, wrt_request_info *info);
+int wrt_server_get_stats(wrt_server *srv, wrt_server_stats *stats);
+/* Finishes the launches in flight, cancels queued requests
+ * (WRT_ERR_CANCELLED) and releases everything. */
+int wrt_server_destroy(wrt_server *srv);
 
 /* ------------------------------------------------------------ measurement */
 /* CUDA-event timer on the context's stream: start records an event, stop

@@ -46,6 +46,38 @@ class PlaneOpts(C.Structure):
                 ("reserved", C.c_int * 5)]
 
 
+class ForwardReq(C.Structure):
+    _fields_ = [("volume", C.c_void_p), ("grid", C.c_void_p), ("half_extent", C.c_int),
+                ("reserved", C.c_int), ("dev_out", C.c_void_p)]
+
+
+OP_FORWARD, OP_ADJOINT = 0, 1
+
+
+class Request(C.Structure):
+    _fields_ = [("op", C.c_int), ("ngrid", C.c_int), ("nphi", C.c_int), ("ntheta", C.c_int),
+                ("nshift", C.c_int), ("half_extent", C.c_int), ("volume", C.c_void_p),
+                ("radon", C.c_void_p), ("out", C.c_void_p), ("tag", C.c_uint64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("batch_size", C.c_int), ("tag", C.c_uint64),
+                ("submit_ms", C.c_double), ("start_ms", C.c_double), ("done_ms", C.c_double)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("max_batch", C.c_int), ("max_inflight", C.c_int),
+                ("queue_capacity", C.c_int), ("hbm_budget", C.c_size_t),
+                ("reserved", C.c_int * 8)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("launches", C.c_uint64), ("budget", C.c_size_t), ("bytes_in_use", C.c_size_t),
+                ("bytes_peak", C.c_size_t), ("queued", C.c_size_t), ("in_flight", C.c_size_t),
+                ("grid_shapes", C.c_size_t)]
+
+
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _vp, _i, _sz = C.c_void_p, C.c_int, C.c_size_t
@@ -105,6 +137,12 @@ def lib() -> C.CDLL:
         L.wrt_plane_kernel_config_describe.argtypes = [_i, C.POINTER(_i), C.POINTER(_i),
                                                        C.POINTER(_i)]
         L.wrt_ctx_set_plane_kernel_config.argtypes = [_vp, _i]
+        L.wrt_radon_forward_batch.argtypes = [_vp, C.POINTER(ForwardReq), _i]
+        L.wrt_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(_vp)]
+        L.wrt_server_submit.argtypes = [_vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
+        L.wrt_server_wait.argtypes = [_vp, C.c_uint64, _i, C.POINTER(RequestInfo)]
+        L.wrt_server_get_stats.argtypes = [_vp, C.POINTER(ServerStats)]
+        L.wrt_server_destroy.argtypes = [_vp]
         _lib = L
     return _lib
 
@@ -402,3 +440,92 @@ def tune_plane_kernel(ctx: Context, vol: Volume, grid: Grid, dev_out: int, sampl
     ctx.check(lib().wrt_tune_plane_kernel(ctx.handle, vol.handle, grid.handle, C.byref(o),
                                           _vp(dev_out), C.byref(best), C.byref(ms)), "tune")
     return best.value, float(ms.value)
+
+
+def radon_forward_batch(ctx: Context, requests):
+    """One launch for many forward requests.  ``requests``: sequence of
+    (Volume, Grid, dev_out pointer, half_extent) tuples; asynchronous on the
+    context's stream (trilinear sampler, staged kernel)."""
+    arr = (ForwardReq * max(1, len(requests)))()
+    for k, (vol, grid, dev_out, half_extent) in enumerate(requests):
+        arr[k].volume = vol.handle.value
+        arr[k].grid = grid.handle.value
+        arr[k].half_extent = int(half_extent or 0)
+        arr[k].dev_out = int(dev_out)
+    ctx.check(lib().wrt_radon_forward_batch(ctx.handle, arr, len(requests)), "radon_forward_batch")
+
+
+class Server:
+    """The serving loop (wrt_server): submit forward / adjoint requests from
+    host arrays, wait for them by id.  The arrays passed to ``submit`` are kept
+    alive here until the request has been waited for."""
+
+    def __init__(self, device: int = 0, max_batch: int = 0, max_inflight: int = 0,
+                 budget_bytes: int = 0, queue_capacity: int = 0):
+        o = ServerOpts()
+        o.device, o.max_batch, o.max_inflight = int(device), int(max_batch), int(max_inflight)
+        o.queue_capacity, o.hbm_budget = int(queue_capacity), int(budget_bytes)
+        self._h = _vp()
+        st = lib().wrt_server_create(C.byref(o), C.byref(self._h))
+        if st:
+            raise WrtError(st, "wrt_server_create")
+        self._keep = {}
+
+    def submit_forward(self, volume, nphi, ntheta, nshift, out, half_extent=0, tag=0) -> int:
+        """volume: float32 [n][n][n]; out: float64 [nshift][nphi][ntheta]."""
+        v = np.ascontiguousarray(volume, dtype=np.float32)
+        assert out.flags.c_contiguous and out.dtype == np.float64
+        assert out.size == nshift * nphi * ntheta
+        r = Request(OP_FORWARD, v.shape[0], nphi, ntheta, nshift, int(half_extent),
+                    v.ctypes.data, None, out.ctypes.data, int(tag))
+        return self._submit(r, (v, out))
+
+    def submit_adjoint(self, radon, ngrid, out, tag=0) -> int:
+        """radon: float64 [nshift][nphi][ntheta]; out: float64 [n][n][n] ([iz][ix][iy])."""
+        g = np.ascontiguousarray(radon, dtype=np.float64)
+        nshift, nphi, ntheta = g.shape
+        assert out.flags.c_contiguous and out.dtype == np.float64 and out.size == ngrid ** 3
+        r = Request(OP_ADJOINT, int(ngrid), nphi, ntheta, nshift, 0, None, g.ctypes.data,
+                    out.ctypes.data, int(tag))
+        return self._submit(r, (g, out))
+
+    def _submit(self, r, keep) -> int:
+        rid = C.c_uint64()
+        st = lib().wrt_server_submit(self._h, C.byref(r), C.byref(rid))
+        if st:
+            raise WrtError(st, "wrt_server_submit")
+        self._keep[rid.value] = keep
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> RequestInfo:
+        info = RequestInfo()
+        st = lib().wrt_server_wait(self._h, int(rid), int(timeout_ms), C.byref(info))
+        if st == 6:  # still running
+            raise TimeoutError(rid)
+        self._keep.pop(rid, None)
+        if st:
+            raise WrtError(st, f"request {rid}")
+        return info
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        lib().wrt_server_get_stats(self._h, C.byref(s))
+        return s
+
+    def close(self):
+        if self._h:
+            lib().wrt_server_destroy(self._h)
+            self._h = _vp()
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -200,6 +200,12 @@ int wrt_ctx_destroy(wrt_ctx *ctx) {
   ctx_free(ctx, ctx->flush_buf, ctx->flush_bytes);
   ctx_free(ctx, ctx->d_counter, sizeof(unsigned long long));
   for (auto &kv : ctx->user_allocs) cudaFree(kv.first);
+  if (ctx->batch_slot) {
+    BatchSlot *s = static_cast<BatchSlot *>(ctx->batch_slot);
+    batch_slot_release(s);
+    delete s;
+    ctx->batch_slot = nullptr;
+  }
   staged_release(ctx);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -509,12 +515,12 @@ int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, in
   r.nshift = grid->nshift;
   r.L = L;
   r.guard = 6.0e-7f * (float)(n > 64 ? n : 64);
-  const double rc = sqrt((double)vol->r2) + sampler_margin(n, WRT_SAMPLER_TRILINEAR);
-  r.crop_r2 = (float)fmin(rc * rc * (1.0 + 1e-6), 3.0 + 1e-5);
+  r.crop_r2 = trilinear_crop_r2(vol->r2, n);
   r.scale = fixed_point_scale(vol->maxabs, L);
   StagedItem *d_items = nullptr;
+  const int *d_nitems = nullptr;
   int nitems = 0;
-  st = staged_items_cached(ctx, n, th, r.crop_r2, r.ndir, &d_items, &nitems);
+  st = staged_items_cached(ctx, n, th, r.crop_r2, r.ndir, &d_items, &d_nitems, &nitems);
   if (st) return st;
   st = staged_scratch(ctx, sizeof(StagedReq));
   if (st) return st;
@@ -524,8 +530,8 @@ int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, in
   cudaError_t e = cudaMemsetAsync(dev_out, 0, sizeof(double) * nout, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged output reset");
   if (nitems > 0) {
-    st = plane_staged_launch(ctx, (const StagedReq *)ctx->staged_req, d_items, nitems, smem,
-                             ctx->staged_next);
+    st = plane_staged_launch(ctx, ctx->stream, (const StagedReq *)ctx->staged_req, d_items,
+                             d_nitems, smem, ctx->staged_next);
     if (st) return st;
   }
   const double delta = 1.0 / n;
@@ -566,6 +572,57 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const wrt_gri
   job.out = dev_out;
   job.counter = ctx->d_counter;
   return plane_forward_plain(ctx, job);
+}
+
+int wrt_radon_forward_batch(wrt_ctx *ctx, const wrt_forward_req *reqs, int nreq) {
+  if (!ctx || (nreq > 0 && !reqs) || nreq < 0) return WRT_ERR_INVALID_ARGUMENT;
+  if (nreq > kBatchMaxFwd)
+    return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "batch: at most %d requests", kBatchMaxFwd);
+  int st = set_device(ctx);
+  if (st) return st;
+  if (nreq == 0) return WRT_OK;
+  BatchBuilder b;
+  for (int r = 0; r < nreq; ++r) {
+    wrt_volume *vol = const_cast<wrt_volume *>(reqs[r].volume);
+    const wrt_grid *grid = reqs[r].grid;
+    if (!vol || !grid || !reqs[r].dev_out || vol->ctx != ctx || grid->ctx != ctx)
+      return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "batch request %d: bad volume, grid or output", r);
+    const int n = vol->n;
+    int th = 0, qp = 0;
+    if (n < 4 || staged_smem_bytes(n, &th, &qp) <= 0)
+      return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "batch request %d: volume edge %d unsupported", r, n);
+    if (reqs[r].half_extent < 0 || reqs[r].half_extent > 8 * n)
+      return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "batch request %d: bad half extent", r);
+    st = volume_ensure_pairs(vol);
+    if (st) return st;
+    const int L = reqs[r].half_extent ? reqs[r].half_extent : 2 * n;
+    StagedReq q;
+    staged_request(n, vol->pitch, grid->nphi * grid->ntheta, grid->nshift, L, vol->d_pairs,
+                   vol->d_vol, grid->d_dir, grid->d_dir32, grid->d_shift, grid->d_shift32,
+                   reqs[r].dev_out, &q);
+    FwdAux a = {};
+    a.vol = vol->d_vol;
+    a.pairs = vol->d_pairs;
+    a.stats = vol->d_stats;
+    a.nout = (long long)q.ndir * q.nshift;
+    a.n = n;
+    a.pitch = vol->pitch;
+    a.L = L;
+    a.prep = 0;
+    batch_add_forward(b, q, a, trilinear_crop_r2(vol->r2, n));
+  }
+  if (!ctx->batch_slot) {
+    BatchSlot *s = new (std::nothrow) BatchSlot();
+    if (!s) return WRT_ERR_OUT_OF_MEMORY;
+    st = batch_slot_init(ctx, s, ctx->stream);
+    if (st) {
+      batch_slot_release(s);
+      delete s;
+      return st;
+    }
+    ctx->batch_slot = s;
+  }
+  return batch_slot_launch(static_cast<BatchSlot *>(ctx->batch_slot), b);
 }
 
 int wrt_plane_kernel_config_count(void) { return kNumStagedConfigs; }

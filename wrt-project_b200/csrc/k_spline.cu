@@ -14,6 +14,7 @@
 // the same piecewise cubic as the reference's spline.
 #include <vector>
 
+#include "spline_dev.cuh"
 #include "wrt_internal.cuh"
 
 namespace {
@@ -31,33 +32,8 @@ __global__ void spline_prep_kernel(const double *__restrict__ src, int nlines, i
   const int L = blockIdx.x * blockDim.x + threadIdx.x;
   if (L >= nlines) return;
   const int outer = L / ninner, inner = L % ninner;
-  const double *y = src + outer * so + inner * si;
-  double *M = scratch + (size_t)L * ns;
-  // forward sweep: M holds the modified right-hand sides
-  M[0] = 0.0;
-  M[ns - 1] = 0.0;
-  const double six_h2 = 6.0 / (h * h);
-  double prev = 0.0;
-  for (int i = 1; i + 1 < ns; ++i) {
-    double rhs = six_h2 * (y[(i + 1) * se] - 2.0 * y[i * se] + y[(i - 1) * se]);
-    double dpi = (rhs - (i > 1 ? prev : 0.0)) / den[i];
-    M[i] = dpi;
-    prev = dpi;
-  }
-  for (int i = ns - 3; i >= 1; --i) M[i] = M[i] - cp[i] * M[i + 1];
-  float4 *o = out + (size_t)L * (ns - 1);
-  for (int i = 0; i + 1 < ns; ++i)
-    o[i] = make_float4((float)y[i * se], (float)y[(i + 1) * se], (float)M[i], (float)M[i + 1]);
-}
-
-__device__ __forceinline__ float spline_eval(const float4 *__restrict__ line, int ns, float q,
-                                             float h2_6) {
-  // q = (s + 1)/h in knot units
-  float fi = floorf(q);
-  fi = fminf(fmaxf(fi, 0.0f), (float)(ns - 2));
-  const float b = q - fi, a = 1.0f - b;
-  const float4 c = __ldg(line + (int)fi);
-  return fmaf(a, c.x, b * c.y) + ((a * a - 1.0f) * a * c.z + (b * b - 1.0f) * b * c.w) * h2_6;
+  wrtd::spline_line(src + outer * so + inner * si, se, ns, h, cp, den, scratch + (size_t)L * ns,
+                    out + (size_t)L * (ns - 1));
 }
 
 // Reduction: one thread per Radon sample (is, iphi, itheta), order of
@@ -102,10 +78,10 @@ __global__ void __launch_bounds__(256)
     const float f = (float)((z - z0) / delta_z);
     const float q = (float)(s + 1.0) * inv_hs;
     const float4 *l0 = lines + ((size_t)iz * nphi + ip) * line_len;
-    const float v0 = spline_eval(l0, ns_ray, q, h2_6);
-    const float v1 = spline_eval(l0 + (size_t)nphi * line_len, ns_ray, q, h2_6);
+    const float v0 = wrtd::spline_eval(l0, ns_ray, q, h2_6);
+    const float v1 = wrtd::spline_eval(l0 + (size_t)nphi * line_len, ns_ray, q, h2_6);
     const float v2 =
-        iz >= ngrid - 2 ? 0.0f : spline_eval(l0 + 2 * (size_t)nphi * line_len, ns_ray, q, h2_6);
+        iz >= ngrid - 2 ? 0.0f : wrtd::spline_eval(l0 + 2 * (size_t)nphi * line_len, ns_ray, q, h2_6);
     // quadratic through (z0, v0), (z0+dz, v1), (z0+2dz, v2) at z0 + f dz
     const float val = v0 + f * (v1 - v0) + 0.5f * f * (f - 1.0f) * (v2 - 2.0f * v1 + v0);
     acc += (double)val;
@@ -121,27 +97,7 @@ __global__ void __launch_bounds__(256)
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long total = (long long)n * n * n;
   if (k >= total) return;
-  const int iy = (int)(k % n), ix = (int)((k / n) % n), iz = (int)(k / ((long long)n * n));
-  // cell centres, radon3d_ajoint.c:248-250
-  const float x = (float)((-1.0) + (1.0 / n) + ix * (2.0 / n));
-  const float y = (float)((-1.0) + (1.0 / n) + iy * (2.0 / n));
-  const float z = (float)((-1.0) + (1.0 / n) + iz * (2.0 / n));
-  const float hs = 2.0f / (float)(ns - 1);
-  const float inv_hs = 1.0f / hs;
-  const float h2_6 = hs * hs / 6.0f;
-  const size_t line_len = (size_t)(ns - 1);
-  double acc = 0.0;
-  for (int d0 = 0; d0 < ndir; d0 += ntheta) {
-    float part = 0.0f;
-    const int d1 = min(ndir, d0 + ntheta);
-    for (int d = d0; d < d1; ++d) {
-      const float4 w = __ldg(dirw + d);
-      const float s = fmaf(x, w.x, fmaf(y, w.y, z * w.z));
-      if (fabsf(s) <= 1.0f) part = fmaf(w.w, spline_eval(lines + d * line_len, ns, (s + 1.0f) * inv_hs, h2_6), part);
-    }
-    acc += (double)part;
-  }
-  out[k] = acc;
+  out[k] = wrtd::adjoint_voxel(lines, ndir, ntheta, ns, dirw, n, k);
 }
 
 int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long long so,

@@ -8,25 +8,35 @@
 //
 //   work item = (request, z-layer iz, y-tile, chunk of directions).
 //   The CTA stages the layer pair (iz, iz+1) of its y-tile into shared memory
-//   as one float4 per cell (x, y):
-//       (v0, v1 - v0, v0(x+1) - v0, (v1 - v0)(x+1) - (v1 - v0))
+//   as one float4 per (cell x, node row y):
+//       (v0, v0(x+1) - v0, v1 - v0, (v1 - v0)(x+1) - (v1 - v0))
 //   (v0/v1 = node values on layers iz/iz+1), so a trilinear sample is two
-//   16-byte loads (rows y and y+1) and eight FMAs.  Its warps then take the
+//   16-byte loads (node rows y and y+1) and a handful of FMAs.  Two cells of
+//   zeros pad every staged row on both sides in x, so samples just outside
+//   the cube's x faces read zeros and need no bounds test.  The warps take the
 //   chunk's directions one at a time, enumerate every lattice row (shift s,
-//   index i) of that direction whose z falls in layer iz, and walk them with
-//   one lane per row.
+//   index i) of that direction whose z falls in layer iz, and walk each row
+//   with all 32 lanes on consecutive samples (neighbouring lanes read the
+//   same or adjacent cells: broadcasts, few bank conflicts).
 //   Persistent CTAs (one per SM) pull items from a global counter; the host
 //   orders items by estimated cost, largest first.
+//
+// Arithmetic: coordinates and interpolation use the packed FP32 pair
+// instructions of sm_100 (fma/add/sub .f32x2) on (x, y) and on the quad
+// halves.
 //
 // Numerics (same contract as the plain kernel, wrt_internal.cuh): FP32 cell
 // coordinates; a sample whose x or y cell fraction, or a row whose z cell
 // fraction, lies within the guard band of a cell boundary is re-evaluated with
-// the reference's FP64 arithmetic from global memory.  Every row belongs to
-// exactly one layer and every sample to exactly one tile, decided by the same
-// FP32 expressions everywhere.  Row sums are FP64; they are accumulated per
-// plane as 64-bit fixed-point integers (scale 2^k chosen from max|f| so that no
-// sum can overflow), which makes the result independent of the order in which
-// items, warps and atomics complete: bitwise identical alone or in a batch.
+// the reference's FP64 arithmetic from global memory (in a second pass over
+// the rows that have such samples, outside the hot loop).  Every row belongs
+// to exactly one layer and every sample to exactly one tile, decided by the
+// same FP32 expressions everywhere.  A lane sums its samples of one plane in
+// FP32, the warp combines the lanes in a fixed tree, and the plane's sums
+// over items are accumulated as 64-bit fixed-point integers (scale 2^k from
+// max|f| so that no sum can overflow): the result does not depend on the
+// order in which items and atomics complete -- bitwise identical alone or in
+// a batch.
 #include <math.h>
 #include <string.h>
 
@@ -44,6 +54,37 @@ constexpr unsigned kFull = 0xffffffffu;
 // (|x| < 2^22); subtracting the constant's bit pattern recovers it.
 constexpr float kMagic = 12582912.0f;
 constexpr int kMagicBits = 0x4B400000;
+constexpr int kPadX = 2;  // zero cells staged left and right of every row
+
+// ---- packed FP32 pairs (f32x2 arithmetic of sm_100)
+typedef unsigned long long u64;
+__device__ __forceinline__ u64 pk2(float lo, float hi) {
+  u64 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk2(u64 r, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(r));
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+  u64 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ u64 add2(u64 a, u64 b) {
+  u64 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ u64 sub2(u64 a, u64 b) {
+  u64 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+// 16-byte shared-memory load as two pairs, 32-bit shared address
+__device__ __forceinline__ void lds_pairs(unsigned addr, u64 &lo, u64 &hi) {
+  asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(lo), "=l"(hi) : "r"(addr));
+}
 
 __device__ __forceinline__ float row_w(float s, float nz, float a1z, float di, float h) {
   return (fmaf(di, a1z, s * nz) + 1.0f) * h;
@@ -71,18 +112,20 @@ __device__ __forceinline__ int rows_in_layer(float s, float nz, float a1z, float
   return b >= a ? b - a + 1 : 0;
 }
 
-__device__ __forceinline__ bool clip_lin(float q0, float dq, float lo, float hi, int &jlo,
-                                         int &jhi) {
-  // conservative j-range with q0 + j dq in [lo, hi]
+// j-range with q0 + j dq in [lo, hi] (inv = 1/dq), widened by less than one
+// sample on each side: with |dq| < 1/2 the samples kept lie within half a cell
+// of [lo, hi] (the staged rows' zero padding relies on this).
+__device__ __forceinline__ bool clip_lin(float q0, float dq, float inv, float lo, float hi,
+                                         int &jlo, int &jhi) {
   if (dq == 0.0f) return q0 >= lo && q0 <= hi;
-  float a = (lo - q0) / dq, b = (hi - q0) / dq;
+  float a = (lo - q0) * inv, b = (hi - q0) * inv;
   if (a > b) {
-    float t = a;
+    const float t = a;
     a = b;
     b = t;
   }
-  a = fmaxf(a, (float)jlo) - 1.0f;
-  b = fminf(b, (float)jhi) + 1.0f;
+  a = fmaxf(a, (float)jlo) - 0.25f;
+  b = fminf(b, (float)jhi) + 0.25f;
   jlo = max(jlo, (int)floorf(a));
   jhi = min(jhi, (int)ceilf(b));
   return jlo <= jhi;
@@ -106,19 +149,46 @@ __device__ __noinline__ double exact_sample(const wrt::StagedReq &R, int d, int 
   return wrtd::exact_trilinear(R.vol, R.n, px, py, pz);
 }
 
-// kThreads: CTA size (one CTA per SM); kGroup: rows a warp walks together
-// (32/kGroup lanes per row); kShiftsPerLane: shifts a lane enumerates per
-// pass (a pass covers 32*kShiftsPerLane shifts).
-template <int kThreads, int kGroup, int kShiftsPerLane>
+// Sample classification shared by the fast walk and the guard-band walk (the
+// two must agree bit for bit).  q = (x, y) cell coordinates minus 1/2.
+struct SampleC {
+  u64 s;       // q + 1.5 * 2^23 (integer cells in the low mantissa bits)
+  u64 t;       // cell fractions (tx, ty)
+  bool band;   // within the guard band in x or y
+};
+__device__ __forceinline__ SampleC classify(u64 q, u64 magic2, u64 half2, float halfband) {
+  SampleC c;
+  c.s = add2(q, magic2);
+  const u64 d = sub2(q, sub2(c.s, magic2));  // q - round(q), in [-1/2, 1/2]
+  c.t = add2(d, half2);
+  float dx, dy;
+  upk2(d, dx, dy);
+  c.band = fmaxf(fabsf(dx), fabsf(dy)) > halfband;
+  return c;
+}
+
+// kThreads: CTA size (one CTA per SM); kGroup: lattice rows a warp walks at
+// once (32/kGroup lanes per row, on consecutive samples); kShiftsPerLane:
+// shifts a lane enumerates per pass (a pass covers 32*kShiftsPerLane shifts);
+// kCount: count the samples evaluated (measurement build).
+template <int kThreads, int kGroup, int kShiftsPerLane, bool kCount>
 __global__ void __launch_bounds__(kThreads, 1)
     plane_staged_kernel(const wrt::StagedReq *__restrict__ reqs,
-                        const wrt::StagedItem *__restrict__ items, int nitems,
-                        int *__restrict__ next_item, unsigned long long *__restrict__ counter) {
+                        const wrt::StagedItem *__restrict__ items,
+                        const int *__restrict__ nitems_ptr, int *__restrict__ next_item,
+                        unsigned long long *__restrict__ counter) {
   constexpr int kLanesPerRow = 32 / kGroup;
+  constexpr int kWarps = kThreads / 32;
   extern __shared__ float4 quads[];
   __shared__ int s_item, s_dir;
-  const int tid = threadIdx.x, lane = tid & 31;
+  __shared__ unsigned char s_rowlane[kWarps][32];  // compacted non-empty rows -> lane
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int pos = lane % kLanesPerRow;  // position of this lane within its row
+  const unsigned smem0 = (unsigned)__cvta_generic_to_shared(quads);
   unsigned long long evaluated = 0;
+  const u64 magic2 = pk2(kMagic, kMagic), half2 = pk2(0.5f, 0.5f);
+  const u64 step2 = pk2((float)kLanesPerRow, (float)kLanesPerRow);
+  const int nitems = __ldg(nitems_ptr);
   for (;;) {
     if (tid == 0) {
       s_item = atomicAdd(next_item, 1);
@@ -133,16 +203,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int qp = R.qpitch;
     const int y0 = item.tile * R.tile_h;
     const int H = min(R.tile_h, W - y0);
-    // ---- stage layer pair (iz, iz+1), quad rows y0 .. y0+H
+    // ---- stage layer pair (iz, iz+1), node rows y0 .. y0+H, cells -2 .. W+1
     {
       const float2 *src = R.pairs + (size_t)item.layer * n * R.pitch2 + (size_t)y0 * R.pitch2;
-      const int total = (H + 1) * W;
+      const int wide = W + 2 * kPadX;
+      const int total = (H + 1) * wide;
       for (int k = tid; k < total; k += kThreads) {
-        const int yy = k / W, x = k - yy * W;
-        const float2 *row = src + (size_t)yy * R.pitch2;
-        const float2 a = __ldg(row + x), b = __ldg(row + x + 1);
-        const float dz0 = a.y - a.x, dz1 = b.y - b.x;
-        quads[yy * qp + x] = make_float4(a.x, dz0, b.x - a.x, dz1 - dz0);
+        const int yy = k / wide, xc = k - yy * wide, x = xc - kPadX;
+        float4 q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (x >= 0 && x < W) {
+          const float2 *row = src + (size_t)yy * R.pitch2;
+          const float2 a = __ldg(row + x), b = __ldg(row + x + 1);
+          const float dz0 = a.y - a.x, dz1 = b.y - b.x;
+          q = make_float4(a.x, b.x - a.x, dz0, dz1 - dz0);
+        }
+        quads[yy * qp + xc] = q;
       }
     }
     __syncthreads();
@@ -154,6 +229,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const float whi = item.layer == W - 1 ? (float)W + g : (float)(item.layer + 1);
     const float rc2 = R.crop_r2;
     const int L = R.L;
+    // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x + magic))
+    const unsigned sbase = smem0 + 16u * (unsigned)(kPadX - kMagicBits);
+    const unsigned qp16 = 16u * (unsigned)qp;
+    const int yoff = kMagicBits + y0;
     for (;;) {
       int dl = 0;
       if (lane == 0) dl = atomicAdd(&s_dir, 1);
@@ -171,6 +250,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       D.a2x = __ldg(Df + 6) * delta;
       D.a2y = __ldg(Df + 7) * delta;
       const float du = D.a2x * h, dv = D.a2y * h;
+      const float inv_du = du != 0.0f ? 1.0f / du : 0.0f;
+      const float inv_dv = dv != 0.0f ? 1.0f / dv : 0.0f;
+      const u64 duv = pk2(du, dv);
       for (int sb = 0; sb < R.nshift; sb += 32 * kShiftsPerLane) {
         // ---- enumerate rows of this layer: lane owns shifts sb + lane*K + k
         int cnt[kShiftsPerLane], ia[kShiftsPerLane];
@@ -221,7 +303,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (is < 0) off -= c;
           }
           const bool valid = r < total && is >= 0;
-          // ---- row set-up
+          // ---- row set-up (one lane per row)
           int jlo = 1, jhi = 0;
           float ub = 0.f, vb = 0.f, tz = 0.f;
           bool zexact = false;
@@ -238,88 +320,118 @@ __global__ void __launch_bounds__(kThreads, 1)
               const int jm = (int)floorf(sqrtf(rem) / delta) + 1;
               jlo = max(-L, -jm);
               jhi = min(L - 1, jm);
-              if (!clip_lin(ub, du, -1.0f, (float)n, jlo, jhi) ||
-                  !clip_lin(vb, dv, (float)y0 - 1.0f, (float)(y0 + H) + 1.0f, jlo, jhi)) {
+              if (!clip_lin(ub, du, inv_du, -1.0f, (float)n, jlo, jhi) ||
+                  !clip_lin(vb, dv, inv_dv, (float)y0 - 1.0f, (float)(y0 + H) + 1.0f, jlo, jhi)) {
                 jlo = 1;
                 jhi = 0;
               }
             }
           }
-          // ---- walk the rows in groups of kGroup, kLanesPerRow lanes per row,
-          // consecutive samples on consecutive lanes of a row
-          const int nrows = min(32, total - r0);
+          // ---- compact the non-empty rows (in row order) and walk them kGroup at a time
+          const bool live_row = valid && jlo <= jhi;
+          const unsigned rows = __ballot_sync(kFull, live_row);
+          const int nrows = __popc(rows);
+          if (live_row) s_rowlane[warp][__popc(rows & ((1u << lane) - 1u))] = (unsigned char)lane;
+          __syncwarp();
           for (int g0 = 0; g0 < nrows; g0 += kGroup) {
-            const int rr = g0 + lane / kLanesPerRow, pos = lane % kLanesPerRow;
-            const bool rvalid = rr < nrows;
-            const int src = rvalid ? rr : 0;
+            const int kr = g0 + lane / kLanesPerRow;
+            const bool rvalid = kr < nrows;
+            const int src = rvalid ? s_rowlane[warp][kr] : 0;
             const int k_is = __shfl_sync(kFull, is, src), k_i = __shfl_sync(kFull, i, src);
+            // (every lane takes part in every shuffle; the row's validity is
+            // applied afterwards)
             const int k_jlo = __shfl_sync(kFull, jlo, src);
             const int jhi_src = __shfl_sync(kFull, jhi, src);
-            const int k_jhi = rvalid ? jhi_src : k_jlo - 1;
             const float k_ubm = __shfl_sync(kFull, ub, src) - 0.5f;  // q - 1/2 at j = 0
             const float k_vbm = __shfl_sync(kFull, vb, src) - 0.5f;
             const float k_tz = __shfl_sync(kFull, tz, src);
-            const bool k_zx = __shfl_sync(kFull, (int)zexact, src) != 0;
-            const int len = max(0, k_jhi - k_jlo + 1);
-            const int trips = (int)__reduce_max_sync(kFull, (unsigned)((len + kLanesPerRow - 1) / kLanesPerRow));
+            const int zx_src = __shfl_sync(kFull, (int)zexact, src);
+            const int k_jhi = rvalid ? jhi_src : k_jlo - 1;
+            const bool k_zx = rvalid && zx_src != 0;
+            const u64 qb = pk2(k_ubm, k_vbm), tz2 = pk2(k_tz, k_tz);
+            const int len = k_jhi - k_jlo + 1;
+            const int trips = (int)__reduce_max_sync(
+                kFull, (unsigned)((max(len, 0) + kLanesPerRow - 1) / kLanesPerRow));
             const float jhif = (float)k_jhi;
-            float jf = (float)(k_jlo + pos);
+            const float jf0 = (float)(k_jlo + pos);
+            bool any_band = k_zx;
             float part = 0.0f;
-            double xacc = 0.0;  // guard-band samples, FP64
-            for (int t = 0; t < trips; ++t, jf += (float)kLanesPerRow) {
-              if (jf <= jhif) {
-                // cell = round-to-nearest(q - 1/2) via the 1.5 * 2^23 shift (no
-                // float-to-int conversion instructions); d = frac(q) - 1/2
-                const float qx = fmaf(jf, du, k_ubm), qy = fmaf(jf, dv, k_vbm);
-                const float sx = qx + kMagic, sy = qy + kMagic;
-                const float fx = sx - kMagic, fy = sy - kMagic;
-                const float dx = qx - fx, dy = qy - fy;
-                const int ix = __float_as_int(sx) - kMagicBits;
-                const int iy = __float_as_int(sy) - kMagicBits - y0;
-                const bool band = k_zx | (fmaxf(fabsf(dx), fabsf(dy)) > halfband);
-                if (!band) {
-                  if ((unsigned)ix < (unsigned)W && (unsigned)iy < (unsigned)H) {
-                    const float tx = dx + 0.5f, ty = dy + 0.5f;
-                    const float4 *q = quads + iy * qp + ix;
-                    const float4 a = q[0], b = q[qp];
-                    const float va = fmaf(tx, fmaf(k_tz, a.w, a.z), fmaf(k_tz, a.y, a.x));
-                    const float vb2 = fmaf(tx, fmaf(k_tz, b.w, b.z), fmaf(k_tz, b.y, b.x));
-                    part += fmaf(ty, vb2 - va, va);
-                    ++evaluated;
-                  }
-                } else {
-                  // a guard-band sample belongs to the tile of its FP32 cell row,
-                  // clamped to the grid (samples within the band outside a face
-                  // are evaluated, and cut off, by the FP64 reference arithmetic)
-                  const int cy = min(max(iy + y0, 0), W - 1) - y0;
-                  if ((unsigned)cy < (unsigned)H) {
-                    xacc += exact_sample(R, d, k_is, k_i, (int)jf);
-                    ++evaluated;
-                  }
+            {
+              u64 jj = pk2(jf0, jf0);
+              for (int t = 0; t < trips; ++t, jj = add2(jj, step2)) {
+                float jf, jf_hi;
+                upk2(jj, jf, jf_hi);
+                const SampleC c = classify(fma2(jj, duv, qb), magic2, half2, halfband);
+                float sx, sy;
+                upk2(c.s, sx, sy);
+                const int iyr = __float_as_int(sy) - yoff;
+                const bool live = jf <= jhif;
+                any_band |= live & c.band;
+                if (live & !(c.band | k_zx) & ((unsigned)iyr < (unsigned)H)) {
+                  const unsigned a = sbase + 16u * (unsigned)(iyr * qp + __float_as_int(sx));
+                  u64 a01, a23, b01, b23;
+                  lds_pairs(a, a01, a23);
+                  lds_pairs(a + qp16, b01, b23);
+                  float ca, cxa, cb, cxb, tx, ty;
+                  upk2(fma2(a23, tz2, a01), ca, cxa);  // (v + tz dz, dv/dx + tz d(dz)/dx)
+                  upk2(fma2(b23, tz2, b01), cb, cxb);
+                  upk2(c.t, tx, ty);
+                  const float va = fmaf(tx, cxa, ca), vb2 = fmaf(tx, cxb, cb);
+                  part += fmaf(ty, vb2 - va, va);
+                  if (kCount) ++evaluated;
                 }
               }
             }
-            // ---- fixed-point accumulation, segmented by plane over the warp
-            // (rows are ordered by shift, so lanes of one plane are contiguous)
-            const double row_acc = xacc + (double)part;
-            long long v = rvalid ? __double2ll_rn(row_acc * R.scale) : 0LL;
+            // ---- guard-band samples (and whole rows in the z band): the
+            // reference's FP64 arithmetic, from global memory
+            double xacc = 0.0;
+            if (__any_sync(kFull, any_band)) {
+              u64 jj = pk2(jf0, jf0);
+              for (int t = 0; t < trips; ++t, jj = add2(jj, step2)) {
+                float jf, jf_hi;
+                upk2(jj, jf, jf_hi);
+                const SampleC c = classify(fma2(jj, duv, qb), magic2, half2, halfband);
+                float sx, sy;
+                upk2(c.s, sx, sy);
+                // a guard-band sample belongs to the tile of its FP32 cell row,
+                // clamped to the grid (samples within the band outside a face
+                // are evaluated, and cut off, by the FP64 reference arithmetic)
+                const int cy = min(max(__float_as_int(sy) - kMagicBits, 0), W - 1) - y0;
+                if ((jf <= jhif) & (c.band | k_zx) & ((unsigned)cy < (unsigned)H)) {
+                  xacc += exact_sample(R, d, k_is, k_i, (int)jf);
+                  if (kCount) ++evaluated;
+                }
+              }
+            }
+            // ---- row sums over the row's lanes, fixed point, then the rows
+            // of one plane combined (rows are in plane order) and one atomic
+            // per plane segment
+#pragma unroll
+            for (int o = kLanesPerRow / 2; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+            if (__any_sync(kFull, xacc != 0.0)) {
+#pragma unroll
+              for (int o = kLanesPerRow / 2; o > 0; o >>= 1) xacc += __shfl_xor_sync(kFull, xacc, o);
+            }
+            long long v = rvalid ? __double2ll_rn(((double)part + xacc) * R.scale) : 0LL;
             const int key = rvalid ? k_is : -1;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
+            for (int o = kLanesPerRow; o < 32; o <<= 1) {
               const long long tv = __shfl_up_sync(kFull, v, o);
               const int k2 = __shfl_up_sync(kFull, key, o);
               if (lane >= o && k2 == key) v += tv;
             }
-            const int knext = __shfl_down_sync(kFull, key, 1);
-            if (rvalid && (lane == 31 || knext != key) && v != 0)
+            const int knext = kLanesPerRow < 32 ? __shfl_down_sync(kFull, key, kLanesPerRow) : -2;
+            const bool last = lane >= 32 - kLanesPerRow || knext != key;
+            if (rvalid && pos == 0 && last && v != 0)
               atomicAdd(R.acc + (size_t)k_is * R.ndir + d, (unsigned long long)v);
           }
+          __syncwarp();
         }
       }
     }
     __syncthreads();
   }
-  if (counter) {
+  if (kCount) {
     for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(kFull, evaluated, o);
     if (lane == 0 && evaluated) atomicAdd(counter, evaluated);
   }
@@ -340,10 +452,10 @@ namespace wrt {
 
 int staged_smem_bytes(int n, int *tile_h, int *qpitch) {
   const int W = n - 1;
-  int qp = W;
+  int qp = W + 2 * kPadX;
   while (qp % 8 != 3) ++qp;  // 16-byte words: rows offset by 3 bank groups
-  const int budget = 200 * 1024;
-  int rows_max = budget / (qp * 16);  // quad rows that fit
+  const int budget = kStagedSmemMax;
+  int rows_max = budget / (qp * 16);  // node rows that fit
   if (rows_max < 3) return -1;
   int ntiles = (W + (rows_max - 1) - 1) / (rows_max - 1);
   int th = (W + ntiles - 1) / ntiles;  // balanced tiles of <= rows_max-1 cells
@@ -354,38 +466,41 @@ int staged_smem_bytes(int n, int *tile_h, int *qpitch) {
 
 namespace {
 template <int T, int G, int K>
-int launch_cfg(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items, int nitems,
-               int max_smem, int *d_next) {
-  cudaError_t e = cudaFuncSetAttribute(plane_staged_kernel<T, G, K>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+int launch_cfg(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
+               const StagedItem *d_items, const int *d_nitems, int max_smem, int *d_next) {
+  const bool count = ctx->d_counter != nullptr;
+  auto kern = count ? plane_staged_kernel<T, G, K, true> : plane_staged_kernel<T, G, K, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged kernel smem attribute");
-  e = cudaMemsetAsync(d_next, 0, sizeof(int), ctx->stream);
+  e = cudaMemsetAsync(d_next, 0, sizeof(int), stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged counter reset");
-  plane_staged_kernel<T, G, K><<<ctx->sm_count, T, max_smem, ctx->stream>>>(
-      d_reqs, d_items, nitems, d_next, ctx->d_counter);
+  kern<<<ctx->sm_count, T, max_smem, stream>>>(d_reqs, d_items, d_nitems, d_next,
+                                               ctx->d_counter);
   ctx->launches++;
   return check_launch(ctx, "plane_staged_kernel");
 }
 }  // namespace
 
-// The tile shapes the autotuner chooses among: (CTA threads, rows per warp
-// group, shifts per lane per enumeration pass).
+// The tile shapes the autotuner chooses among: (CTA threads, lattice rows a
+// warp walks at once, shifts per lane per enumeration pass).
 const StagedConfig kStagedConfigs[] = {
-    {512, 4, 4}, {512, 8, 4}, {512, 2, 4}, {640, 4, 2}, {768, 4, 2}, {768, 8, 2},
+    {768, 8, 2}, {768, 4, 2}, {1024, 8, 2}, {1024, 4, 2}, {768, 2, 2}, {1024, 1, 2}, {512, 8, 4},
 };
 const int kNumStagedConfigs = sizeof(kStagedConfigs) / sizeof(kStagedConfigs[0]);
 
-int plane_staged_launch(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items,
-                        int nitems, int max_smem, int *d_next) {
+int plane_staged_launch(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
+                        const StagedItem *d_items, const int *d_nitems, int max_smem,
+                        int *d_next) {
   const int c = (ctx->staged_config >= 0 && ctx->staged_config < kNumStagedConfigs)
                     ? ctx->staged_config : 0;
   switch (c) {
-    case 0: return launch_cfg<512, 4, 4>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
-    case 1: return launch_cfg<512, 8, 4>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
-    case 2: return launch_cfg<512, 2, 4>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
-    case 3: return launch_cfg<640, 4, 2>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
-    case 4: return launch_cfg<768, 4, 2>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
-    default: return launch_cfg<768, 8, 2>(ctx, d_reqs, d_items, nitems, max_smem, d_next);
+    case 0: return launch_cfg<768, 8, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 1: return launch_cfg<768, 4, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 2: return launch_cfg<1024, 8, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 3: return launch_cfg<1024, 4, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 4: return launch_cfg<768, 2, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 5: return launch_cfg<1024, 1, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    default: return launch_cfg<512, 8, 4>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
   }
 }
 
@@ -398,16 +513,11 @@ int plane_finalize(wrt_ctx *ctx, double *out, long long count, double factor) {
 
 // Work items of one request, largest estimated cost first.  Cost of a
 // (layer, tile): voxels of the tile's slab inside the crop radius.
-void staged_items(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
-                  std::vector<StagedItem> &out) {
+void staged_items_costed(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
+                         double weight, std::vector<std::pair<double, StagedItem>> &out) {
   const int W = n - 1;
   const int ntiles = (W + tile_h - 1) / tile_h;
   const double h = 2.0 / (n - 1);
-  struct C {
-    double cost;
-    StagedItem it;
-  };
-  std::vector<C> v;
   for (int iz = 0; iz < W; ++iz) {
     const double z = -1.0 + h * (iz + 0.5);
     for (int t = 0; t < ntiles; ++t) {
@@ -425,26 +535,25 @@ void staged_items(int req, int n, int tile_h, float crop_r2, int ndir, int dir_c
         it.tile = t;
         it.dir0 = d0;
         it.ndir = std::min(dir_chunk, ndir - d0);
-        v.push_back({cost * it.ndir, it});
+        out.push_back({cost * it.ndir * weight, it});
       }
     }
   }
-  std::stable_sort(v.begin(), v.end(), [](const C &a, const C &b) { return a.cost > b.cost; });
-  for (auto &c : v) out.push_back(c.it);
 }
 
-double fixed_point_scale(float maxabs, int L) {
-  // |row sum| <= maxabs * 2L and |plane sum| <= maxabs * (2L)^2: scale so the
-  // plane sum stays below 2^61 in magnitude
-  if (!(maxabs > 0.0f) || !isfinite(maxabs)) return 1.0;
-  const double bound = (double)maxabs * (2.0 * L + 1.0) * (2.0 * L + 1.0);
-  const int k = (int)floor(log2(ldexp(1.0, 61) / bound));
-  return ldexp(1.0, std::max(-200, std::min(200, k)));
+void staged_items(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
+                  std::vector<StagedItem> &out) {
+  std::vector<std::pair<double, StagedItem>> v;
+  staged_items_costed(req, n, tile_h, crop_r2, ndir, dir_chunk, 1.0, v);
+  std::stable_sort(v.begin(), v.end(),
+                   [](const std::pair<double, StagedItem> &a,
+                      const std::pair<double, StagedItem> &b) { return a.first > b.first; });
+  for (auto &c : v) out.push_back(c.second);
 }
 
 namespace {
 struct ItemList {
-  StagedItem *d = nullptr;
+  void *d = nullptr;
   int count = 0;
   size_t bytes = 0;
 };
@@ -453,8 +562,10 @@ struct StagedCache {
 };
 }  // namespace
 
+// Device copy of the item list of one geometry: a 16-byte header holding the
+// item count (the kernel reads it from there), then the items.
 int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir,
-                        StagedItem **d_items, int *nitems) {
+                        StagedItem **d_items, const int **d_nitems, int *nitems) {
   if (!ctx->staged_cache) ctx->staged_cache = new StagedCache();
   StagedCache *c = static_cast<StagedCache *>(ctx->staged_cache);
   unsigned bits;
@@ -468,24 +579,24 @@ int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir
       c->lists.clear();
     }
     std::vector<StagedItem> items;
-    const int chunk = 512;  // directions per item
-    staged_items(0, n, tile_h, crop_r2, ndir, chunk, items);
+    staged_items(0, n, tile_h, crop_r2, ndir, kStagedDirChunk, items);
     ItemList l;
     l.count = (int)items.size();
-    l.bytes = sizeof(StagedItem) * std::max<size_t>(1, items.size());
+    l.bytes = 16 + sizeof(StagedItem) * items.size();
+    std::vector<char> host(l.bytes, 0);
+    memcpy(host.data(), &l.count, sizeof(int));
+    if (!items.empty()) memcpy(host.data() + 16, items.data(), sizeof(StagedItem) * items.size());
     int st = ctx_alloc(ctx, (void **)&l.d, l.bytes);
     if (st) return st;
-    if (!items.empty()) {
-      cudaError_t e = cudaMemcpy(l.d, items.data(), sizeof(StagedItem) * items.size(),
-                                 cudaMemcpyHostToDevice);
-      if (e != cudaSuccess) {
-        ctx_free(ctx, l.d, l.bytes);
-        return cuda_fail(ctx, e, "staged items");
-      }
+    cudaError_t e = cudaMemcpy(l.d, host.data(), l.bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      ctx_free(ctx, l.d, l.bytes);
+      return cuda_fail(ctx, e, "staged items");
     }
     it = c->lists.emplace(key, l).first;
   }
-  *d_items = it->second.d;
+  *d_nitems = reinterpret_cast<const int *>(it->second.d);
+  *d_items = reinterpret_cast<StagedItem *>(reinterpret_cast<char *>(it->second.d) + 16);
   *nitems = it->second.count;
   return WRT_OK;
 }

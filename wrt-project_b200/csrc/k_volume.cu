@@ -23,7 +23,6 @@ template <typename T>
 __global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *__restrict__ dst,
                                       unsigned int *__restrict__ stats) {
   const size_t total = (size_t)n * n * n;
-  const double h = 2.0 / (n - 1);
   float local = 0.0f, amax = 0.0f;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
        k += (size_t)gridDim.x * blockDim.x) {
@@ -31,10 +30,8 @@ __global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *_
     dst[k] = v;
     amax = fmaxf(amax, fabsf(v));
     if (v != 0.0f) {
-      int iz = (int)(k % n), iy = (int)((k / n) % n), ix = (int)(k / ((size_t)n * n));
-      double x = -1.0 + h * ix, y = -1.0 + h * iy, z = -1.0 + h * iz;
-      float r2 = (float)(x * x + y * y + z * z) * (1.0f + 1e-6f);
-      local = fmaxf(local, r2);
+      const int iz = (int)(k % n), iy = (int)((k / n) % n), ix = (int)(k / ((size_t)n * n));
+      local = fmaxf(local, wrtd::node_r2(ix, iy, iz, n));
     }
   }
   // warp max, one atomic per warp

@@ -25,6 +25,7 @@
 #include <stddef.h>
 
 #include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include "../../include/wrt.h"
@@ -53,6 +54,7 @@ struct wrt_ctx {
   int *staged_next = nullptr;
   void *staged_cache = nullptr;
   int staged_config = -1;  // tile configuration (-1: default), set by the autotuner
+  void *batch_slot = nullptr;  // BatchSlot of wrt_radon_forward_batch (batch.cu)
 };
 
 namespace wrt {
@@ -121,16 +123,97 @@ struct StagedConfig {
 extern const StagedConfig kStagedConfigs[];
 extern const int kNumStagedConfigs;
 int staged_smem_bytes(int n, int *tile_h, int *qpitch);
-int plane_staged_launch(wrt_ctx *ctx, const StagedReq *d_reqs, const StagedItem *d_items,
-                        int nitems, int max_smem, int *d_next);
+constexpr int kStagedDirChunk = 512;  // directions per work item
+constexpr int kStagedSmemMax = 200 * 1024;  // staged tile budget (bytes of shared memory)
+int plane_staged_launch(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
+                        const StagedItem *d_items, const int *d_nitems, int max_smem,
+                        int *d_next);
 int plane_finalize(wrt_ctx *ctx, double *out, long long count, double factor);
+// Work items of one request (layer x y-tile x direction chunk) with their
+// estimated cost (staged voxels inside the crop radius x directions x weight).
+void staged_items_costed(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
+                         double weight, std::vector<std::pair<double, StagedItem>> &out);
 void staged_items(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
                   std::vector<StagedItem> &out);
-double fixed_point_scale(float maxabs, int L);
 int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir,
-                        StagedItem **d_items, int *nitems);
+                        StagedItem **d_items, const int **d_nitems, int *nitems);
 int staged_scratch(wrt_ctx *ctx, size_t req_bytes);
 void staged_release(wrt_ctx *ctx);
+
+// Batches (batch.cu): many requests in one launch of a captured CUDA graph.
+// The batch is one table in device memory (layout BatchLayout), uploaded by
+// the graph's first node from a pinned host mirror; every kernel of the graph
+// reads its work from the table, so one captured graph serves every batch.
+constexpr int kBatchMaxFwd = 256;  // forward requests per batch
+constexpr int kBatchMaxAdj = 256;  // adjoint requests per batch
+struct FwdAux {                    // per forward request, beside its StagedReq
+  const float *vol;                // FP32 volume, reference order
+  float2 *pairs;                   // layer pairs (built in the launch when prep)
+  unsigned int *stats;             // [0] r2 bits, [1] max |v| bits (computed when prep)
+  long long nout;                  // nshift * ndir
+  double factor;                   // delta^2 / scale, written by the launch
+  int n, pitch, L, prep;           // prep: build stats and pairs in this launch
+};
+struct AdjReq {                    // one backprojection
+  const double *radon;             // [is][iphi][itheta]
+  const float4 *dirw;              // [ndir]: omega, dphi * w_theta
+  const double *cp, *den;          // spline elimination coefficients [nshift]
+  double *scratch;                 // [ndir][nshift]
+  float4 *lines;                   // [ndir][nshift - 1]
+  double *out;                     // [iz][ix][iy]
+  int ndir, ntheta, nshift, n;
+};
+struct BatchHeader {
+  int nfwd, nadj, nitems, pad;
+};
+constexpr size_t batch_align(size_t x) { return (x + 255) & ~(size_t)255; }
+struct BatchLayout {
+  static constexpr size_t fwd = 256;
+  static constexpr size_t aux = batch_align(fwd + sizeof(StagedReq) * kBatchMaxFwd);
+  static constexpr size_t adj = batch_align(aux + sizeof(FwdAux) * kBatchMaxFwd);
+  static constexpr size_t items = batch_align(adj + sizeof(AdjReq) * kBatchMaxAdj);
+  static size_t bytes(size_t nitems) { return items + sizeof(StagedItem) * nitems; }
+};
+// Host-side description of one batch.
+struct BatchBuilder {
+  std::vector<StagedReq> fwd;
+  std::vector<FwdAux> aux;
+  std::vector<AdjReq> adj;
+  std::vector<std::pair<double, StagedItem>> items;  // cost, item
+  void clear() {
+    fwd.clear();
+    aux.clear();
+    adj.clear();
+    items.clear();
+  }
+};
+// One reusable launch slot: pinned + device tables and the captured graph.
+struct BatchSlot {
+  wrt_ctx *ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  char *h_table = nullptr, *d_table = nullptr;
+  size_t cap = 0;  // table bytes
+  int *d_next = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t copy_node = nullptr;
+  cudaEvent_t done = nullptr;
+  int config = -2;
+  bool counting = false, launched = false;
+};
+// Adds a forward request (staged kernel) to the builder: its descriptor, its
+// auxiliary record and its work items.  crop_items: crop radius^2 used to
+// generate the items (3 covers the whole cube).
+void batch_add_forward(BatchBuilder &b, const StagedReq &req, const FwdAux &aux,
+                       float crop_items);
+int batch_slot_init(wrt_ctx *ctx, BatchSlot *slot, cudaStream_t stream);
+// Waits for the slot's previous launch, writes the table, launches the graph.
+int batch_slot_launch(BatchSlot *slot, BatchBuilder &b);
+void batch_slot_release(BatchSlot *slot);
+// Fills a StagedReq / FwdAux pair for a volume already on the device.
+void staged_request(int n, int pitch, int ndir, int nshift, int L, const float2 *pairs,
+                    const float *vol, const double *dir, const float *dir32,
+                    const double *shift, const float *shift32, double *out, StagedReq *r);
 
 // Ray kernels (k_ray.cu).
 struct RayJob {
@@ -157,6 +240,37 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
 int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
                     const float4 *d_dirw /* [nphi*ntheta]: omega, dphi*w */, int n,
                     double *d_out);
+
+}  // namespace wrt
+
+// ------------------------------------------ shared by host and device code
+namespace wrt {
+
+// Scale 2^k of the staged kernel's 64-bit fixed-point plane sums: |row sum|
+// <= maxabs * 2L and |plane sum| <= maxabs * (2L+1)^2, so 2^k <= 2^61 / that
+// bound keeps every sum below 2^61 in magnitude.  Written with frexp/ldexp
+// only (exact on host and device), so a request gets the same scale whether
+// the host or a kernel computes it.
+__host__ __device__ inline double fixed_point_scale(float maxabs, int L) {
+  if (!(maxabs > 0.0f) || !(maxabs <= 3.4e38f)) return 1.0;
+  const double bound = (double)maxabs * (2.0 * L + 1.0) * (2.0 * L + 1.0);
+  int e = 0;
+  const double m = frexp(bound, &e);     // bound = m 2^e, m in [1/2, 1)
+  const int lg = (m == 0.5) ? e - 1 : e;  // ceil(log2(bound))
+  int k = 61 - lg;
+  k = k < -200 ? -200 : (k > 200 ? 200 : k);
+  return ldexp(1.0, k);
+}
+
+// Squared crop radius of the trilinear sampler for a volume whose non-zero
+// nodes lie within sqrt(r2) of the origin: every lattice point farther than
+// sqrt(r2) plus one cell diagonal of the node grid has eight zero corners.
+// Correctly rounded operations only (same value on host and device).
+__host__ __device__ inline float trilinear_crop_r2(float r2, int n) {
+  const double h = 2.0 / (n - 1);
+  const double rc = sqrt((double)r2) + (sqrt(3.0) * h + 1e-6);
+  return (float)fmin(rc * rc * (1.0 + 1e-6), 3.0 + 1e-5);
+}
 
 }  // namespace wrt
 
@@ -231,6 +345,18 @@ __device__ __forceinline__ float tri32(const float *__restrict__ v, int n, float
   float b0 = lerp32(tx, c001, c101), b1 = lerp32(tx, c011, c111);
   float e0 = lerp32(ty, a0, a1), e1 = lerp32(ty, b0, b1);
   return lerp32(tz, e0, e1);
+}
+
+// Squared radius of node (ix, iy, iz) of the node grid x_i = -1 + 2 i/(n-1)
+// (radon_grid/src/init.c:120-124), widened by 1e-6 relative, as the volume
+// statistics record it (explicit roundings: the same value in every kernel).
+__device__ __forceinline__ float node_r2(int ix, int iy, int iz, int n) {
+  const double h = 2.0 / (n - 1);
+  const double x = __dadd_rn(-1.0, __dmul_rn(h, (double)ix));
+  const double y = __dadd_rn(-1.0, __dmul_rn(h, (double)iy));
+  const double z = __dadd_rn(-1.0, __dmul_rn(h, (double)iz));
+  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+  return __fmul_rn((float)r2, 1.0f + 1e-6f);
 }
 
 __device__ __forceinline__ double warp_sum(double x) {
