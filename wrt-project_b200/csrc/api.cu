@@ -514,7 +514,7 @@ int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, in
   r.ndir = grid->nphi * grid->ntheta;
   r.nshift = grid->nshift;
   r.L = L;
-  r.guard = 6.0e-7f * (float)(n > 64 ? n : 64);
+  r.guard = staged_guard(n, L);
   r.crop_r2 = trilinear_crop_r2(vol->r2, n);
   r.scale = fixed_point_scale(vol->maxabs, L);
   StagedItem *d_items = nullptr;

@@ -196,7 +196,7 @@ void staged_request(int n, int pitch, int ndir, int nshift, int L, const float2 
   r->ndir = ndir;
   r->nshift = nshift;
   r->L = L;
-  r->guard = 6.0e-7f * (float)(n > 64 ? n : 64);
+  r->guard = staged_guard(n, L);
   r->crop_r2 = 3.0f + 1e-5f;
   r->scale = 1.0;
 }

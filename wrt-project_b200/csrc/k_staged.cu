@@ -55,6 +55,11 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr float kMagic = 12582912.0f;
 constexpr int kMagicBits = 0x4B400000;
 constexpr int kPadX = 2;  // zero cells staged left and right of every row
+// Rows whose FP64 z cell coordinate lies within this distance of a node layer
+// take the FP64 reference path: their z is the reference's up to a few FP64
+// roundings, so only rows on a node layer (where the reference's cell index
+// and fraction can disagree) fall in it.
+constexpr double kZBand = 1e-9;
 
 // ---- packed FP32 pairs (f32x2 arithmetic of sm_100)
 typedef unsigned long long u64;
@@ -86,26 +91,31 @@ __device__ __forceinline__ void lds_pairs(unsigned addr, u64 &lo, u64 &hi) {
   asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(lo), "=l"(hi) : "r"(addr));
 }
 
-__device__ __forceinline__ float row_w(float s, float nz, float a1z, float di, float h) {
-  return (fmaf(di, a1z, s * nz) + 1.0f) * h;
+// z cell coordinate of lattice row i of (shift s, direction): w = (s nz + i
+// delta v1z + 1) h, in FP64 with explicit roundings (the same value wherever
+// it is computed: the layer a row belongs to and its z weight agree).
+__device__ __forceinline__ double row_w(double s, double nz, double a1z, double di, double h) {
+  return __dmul_rn(__dadd_rn(__fma_rn(di, a1z, __dmul_rn(s, nz)), 1.0), h);
 }
 
-// Rows i of (direction, shift) whose z cell coordinate w lies in
-// [wlo, whi) -- w decreases with i.  Returns count, first index in *ia.
-__device__ __forceinline__ int rows_in_layer(float s, float nz, float a1z, float h, float wlo,
-                                             float whi, int imin, int imax, int *ia) {
-  if (imin > imax) return 0;
-  // real-valued inverses of w(i) = (s nz + i a1z + 1) h, then exact fix-up
-  const float base = s * nz;
-  float i_hi = ((wlo / h - 1.0f) - base) / a1z;  // w(i) >= wlo  <=>  i <= i_hi
-  float i_lo = ((whi / h - 1.0f) - base) / a1z;  // w(i) <  whi  <=>  i >  i_lo
-  i_hi = fminf(fmaxf(i_hi, (float)imin - 4.0f), (float)imax + 4.0f);
-  i_lo = fminf(fmaxf(i_lo, (float)imin - 4.0f), (float)imax + 4.0f);
-  int a = (int)floorf(i_lo) + 1, b = (int)floorf(i_hi);
-  for (int k = 0; k < 4 && row_w(s, nz, a1z, (float)a, h) >= whi; ++k) ++a;
-  for (int k = 0; k < 4 && row_w(s, nz, a1z, (float)(a - 1), h) < whi; ++k) --a;
-  for (int k = 0; k < 4 && row_w(s, nz, a1z, (float)b, h) < wlo; ++k) --b;
-  for (int k = 0; k < 4 && row_w(s, nz, a1z, (float)(b + 1), h) >= wlo; ++k) ++b;
+// Rows i in [imin, imax] of (direction, shift) whose z cell coordinate w lies
+// in [wlo, whi) -- w decreases with i (a1z = -sin(theta) delta < 0).  Returns
+// the count, first index in *ia.
+__device__ __forceinline__ int rows_in_layer(double s, double nz, double a1z, double inv_a1z,
+                                             double h, double inv_h, double wlo, double whi,
+                                             int imin, int imax, int *ia) {
+  if (imin > imax || !(a1z < 0.0)) return 0;
+  // real-valued inverses of w(i), then exact fix-up with row_w itself
+  const double base = __dmul_rn(s, nz);
+  double i_hi = ((wlo * inv_h - 1.0) - base) * inv_a1z;  // w(i) >= wlo  <=>  i <= i_hi
+  double i_lo = ((whi * inv_h - 1.0) - base) * inv_a1z;  // w(i) <  whi  <=>  i >  i_lo
+  i_hi = fmin(fmax(i_hi, (double)imin - 4.0), (double)imax + 4.0);
+  i_lo = fmin(fmax(i_lo, (double)imin - 4.0), (double)imax + 4.0);
+  int a = (int)floor(i_lo) + 1, b = (int)floor(i_hi);
+  for (int k = 0; k < 4 && row_w(s, nz, a1z, (double)a, h) >= whi; ++k) ++a;
+  for (int k = 0; k < 4 && row_w(s, nz, a1z, (double)(a - 1), h) < whi; ++k) --a;
+  for (int k = 0; k < 4 && row_w(s, nz, a1z, (double)b, h) < wlo; ++k) --b;
+  for (int k = 0; k < 4 && row_w(s, nz, a1z, (double)(b + 1), h) >= wlo; ++k) ++b;
   a = max(a, imin);
   b = min(b, imax);
   *ia = a;
@@ -131,8 +141,8 @@ __device__ __forceinline__ bool clip_lin(float q0, float dq, float inv, float lo
   return jlo <= jhi;
 }
 
-struct DirF {
-  float nx, ny, nz, a1x, a1y, a1z, a2x, a2y;
+struct Dir64 {
+  double nx, ny, nz, a1x, a1y, a1z;  // normal and delta * v1
 };
 
 __device__ __noinline__ double exact_sample(const wrt::StagedReq &R, int d, int is, int i, int j) {
@@ -167,6 +177,19 @@ __device__ __forceinline__ SampleC classify(u64 q, u64 magic2, u64 half2, float 
   return c;
 }
 
+// FP64 reference evaluation of `count` queued guard-band samples of direction
+// d, one per lane, each added to its plane as a fixed-point integer.  Returns
+// the number of samples this lane evaluated.
+__device__ __forceinline__ int exact_queue_flush(const wrt::StagedReq &R, int d,
+                                                 const int2 *q, int count, int lane) {
+  if (lane >= count) return 0;
+  const int2 e = q[lane];
+  const int i = (int)(short)((unsigned)e.y >> 16), j = (int)(short)((unsigned)e.y & 0xFFFFu);
+  const long long v = __double2ll_rn(exact_sample(R, d, e.x, i, j) * R.scale);
+  if (v != 0) atomicAdd(R.acc + (size_t)e.x * R.ndir + d, (unsigned long long)v);
+  return 1;
+}
+
 // kThreads: CTA size (one CTA per SM); kGroup: lattice rows a warp walks at
 // once (32/kGroup lanes per row, on consecutive samples); kShiftsPerLane:
 // shifts a lane enumerates per pass (a pass covers 32*kShiftsPerLane shifts);
@@ -182,6 +205,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ float4 quads[];
   __shared__ int s_item, s_dir;
   __shared__ unsigned char s_rowlane[kWarps][32];  // compacted non-empty rows -> lane
+  // guard-band samples waiting for the FP64 path: (shift index, i << 16 | j)
+  __shared__ int2 s_xq[kWarps][64];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int pos = lane % kLanesPerRow;  // position of this lane within its row
   const unsigned smem0 = (unsigned)__cvta_generic_to_shared(quads);
@@ -221,12 +246,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
     __syncthreads();
-    const float h = 0.5f * (float)W;
     const float delta = 1.0f / (float)n;
     const float g = R.guard;
     const float halfband = 0.5f - g;
-    const float wlo = item.layer == 0 ? -g : (float)item.layer;
-    const float whi = item.layer == W - 1 ? (float)W + g : (float)(item.layer + 1);
+    // layer bounds of the row enumeration; rows within kZBand of a node layer
+    // (or of the cube's z faces) are evaluated exactly
+    const double h64 = 0.5 * (double)W, inv_h64 = 1.0 / h64, delta64 = 1.0 / (double)n;
+    const double wlo = item.layer == 0 ? -kZBand : (double)item.layer;
+    const double whi = item.layer == W - 1 ? (double)W + kZBand : (double)(item.layer + 1);
     const float rc2 = R.crop_r2;
     const int L = R.L;
     // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x + magic))
@@ -239,20 +266,22 @@ __global__ void __launch_bounds__(kThreads, 1)
       dl = __shfl_sync(kFull, dl, 0);
       if (dl >= item.ndir) break;
       const int d = item.dir0 + dl;
-      const float *Df = R.dir32 + 8 * (size_t)d;
-      DirF D;
-      D.nx = __ldg(Df + 0);
-      D.ny = __ldg(Df + 1);
-      D.nz = __ldg(Df + 2);
-      D.a1x = __ldg(Df + 3) * delta;
-      D.a1y = __ldg(Df + 4) * delta;
-      D.a1z = __ldg(Df + 5) * delta;
-      D.a2x = __ldg(Df + 6) * delta;
-      D.a2y = __ldg(Df + 7) * delta;
-      const float du = D.a2x * h, dv = D.a2y * h;
+      const double *Dd = R.dir + 9 * (size_t)d;
+      Dir64 D;
+      D.nx = __ldg(Dd + 0);
+      D.ny = __ldg(Dd + 1);
+      D.nz = __ldg(Dd + 2);
+      D.a1x = __ldg(Dd + 3) * delta64;
+      D.a1y = __ldg(Dd + 4) * delta64;
+      D.a1z = __ldg(Dd + 5) * delta64;
+      const double inv_a1z = D.a1z != 0.0 ? 1.0 / D.a1z : 0.0;
+      // per-sample steps in cell units, rounded once to FP32
+      const float du = (float)(__ldg(Dd + 6) * delta64 * h64);
+      const float dv = (float)(__ldg(Dd + 7) * delta64 * h64);
       const float inv_du = du != 0.0f ? 1.0f / du : 0.0f;
       const float inv_dv = dv != 0.0f ? 1.0f / dv : 0.0f;
       const u64 duv = pk2(du, dv);
+      int xq_n = 0;  // queued guard-band samples of this direction (warp-uniform)
       for (int sb = 0; sb < R.nshift; sb += 32 * kShiftsPerLane) {
         // ---- enumerate rows of this layer: lane owns shifts sb + lane*K + k
         int cnt[kShiftsPerLane], ia[kShiftsPerLane];
@@ -267,7 +296,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const float rem = rc2 - s * s;
             if (rem >= 0.0f) {
               const int im = (int)floorf(sqrtf(rem) / delta) + 1;
-              cnt[k] = rows_in_layer(s, D.nz, D.a1z, h, wlo, whi, max(-L, -im), min(L - 1, im), &ia[k]);
+              cnt[k] = rows_in_layer(__ldg(R.shift + is), D.nz, D.a1z, inv_a1z, h64, inv_h64, wlo,
+                                     whi, max(-L, -im), min(L - 1, im), &ia[k]);
             }
           }
           lane_total += cnt[k];
@@ -309,19 +339,21 @@ __global__ void __launch_bounds__(kThreads, 1)
           bool zexact = false;
           if (valid) {
             const float s = __ldg(R.shift32 + is);
+            const double s64 = __ldg(R.shift + is), di64 = (double)i;
             const float di = (float)i;
-            const float w = row_w(s, D.nz, D.a1z, di, h);
-            tz = w - (float)item.layer;
-            zexact = fabsf(tz - 0.5f) > halfband;
-            ub = (fmaf(di, D.a1x, s * D.nx) + 1.0f) * h;
-            vb = (fmaf(di, D.a1y, s * D.ny) + 1.0f) * h;
+            const double tz64 = row_w(s64, D.nz, D.a1z, di64, h64) - (double)item.layer;
+            tz = (float)tz64;
+            zexact = tz64 < kZBand || tz64 > 1.0 - kZBand;
+            // row origin in cell units, FP64 then rounded once (minus 1/2 applied below)
+            ub = (float)((fma(di64, D.a1x, s64 * D.nx) + 1.0) * h64 - 0.5);
+            vb = (float)((fma(di64, D.a1y, s64 * D.ny) + 1.0) * h64 - 0.5);
             const float rem = rc2 - s * s - (delta * di) * (delta * di);
             if (rem >= 0.0f) {
               const int jm = (int)floorf(sqrtf(rem) / delta) + 1;
               jlo = max(-L, -jm);
               jhi = min(L - 1, jm);
-              if (!clip_lin(ub, du, inv_du, -1.0f, (float)n, jlo, jhi) ||
-                  !clip_lin(vb, dv, inv_dv, (float)y0 - 1.0f, (float)(y0 + H) + 1.0f, jlo, jhi)) {
+              if (!clip_lin(ub, du, inv_du, -1.5f, (float)n - 0.5f, jlo, jhi) ||
+                  !clip_lin(vb, dv, inv_dv, (float)y0 - 1.5f, (float)(y0 + H) + 0.5f, jlo, jhi)) {
                 jlo = 1;
                 jhi = 0;
               }
@@ -342,8 +374,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             // applied afterwards)
             const int k_jlo = __shfl_sync(kFull, jlo, src);
             const int jhi_src = __shfl_sync(kFull, jhi, src);
-            const float k_ubm = __shfl_sync(kFull, ub, src) - 0.5f;  // q - 1/2 at j = 0
-            const float k_vbm = __shfl_sync(kFull, vb, src) - 0.5f;
+            const float k_ubm = __shfl_sync(kFull, ub, src);  // q - 1/2 at j = 0
+            const float k_vbm = __shfl_sync(kFull, vb, src);
             const float k_tz = __shfl_sync(kFull, tz, src);
             const int zx_src = __shfl_sync(kFull, (int)zexact, src);
             const int k_jhi = rvalid ? jhi_src : k_jlo - 1;
@@ -382,9 +414,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
               }
             }
-            // ---- guard-band samples (and whole rows in the z band): the
-            // reference's FP64 arithmetic, from global memory
-            double xacc = 0.0;
+            // ---- guard-band samples (and whole rows in the z band) go to the
+            // warp's queue; full warps of them take the FP64 path below
             if (__any_sync(kFull, any_band)) {
               u64 jj = pk2(jf0, jf0);
               for (int t = 0; t < trips; ++t, jj = add2(jj, step2)) {
@@ -397,9 +428,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                 // clamped to the grid (samples within the band outside a face
                 // are evaluated, and cut off, by the FP64 reference arithmetic)
                 const int cy = min(max(__float_as_int(sy) - kMagicBits, 0), W - 1) - y0;
-                if ((jf <= jhif) & (c.band | k_zx) & ((unsigned)cy < (unsigned)H)) {
-                  xacc += exact_sample(R, d, k_is, k_i, (int)jf);
-                  if (kCount) ++evaluated;
+                const bool want = (jf <= jhif) & (c.band | k_zx) & ((unsigned)cy < (unsigned)H);
+                const unsigned m = __ballot_sync(kFull, want);
+                if (m) {
+                  if (want)
+                    s_xq[warp][xq_n + __popc(m & ((1u << lane) - 1u))] =
+                        make_int2(k_is, (int)(((unsigned)k_i << 16) | ((unsigned)(int)jf & 0xFFFFu)));
+                  xq_n += __popc(m);
+                  __syncwarp();
+                  if (xq_n >= 32) {
+                    evaluated += exact_queue_flush(R, d, s_xq[warp], 32, lane);
+                    if (lane < xq_n - 32) s_xq[warp][lane] = s_xq[warp][lane + 32];
+                    xq_n -= 32;
+                    __syncwarp();
+                  }
                 }
               }
             }
@@ -408,11 +450,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             // per plane segment
 #pragma unroll
             for (int o = kLanesPerRow / 2; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
-            if (__any_sync(kFull, xacc != 0.0)) {
-#pragma unroll
-              for (int o = kLanesPerRow / 2; o > 0; o >>= 1) xacc += __shfl_xor_sync(kFull, xacc, o);
-            }
-            long long v = rvalid ? __double2ll_rn(((double)part + xacc) * R.scale) : 0LL;
+            long long v = rvalid ? __double2ll_rn((double)part * R.scale) : 0LL;
             const int key = rvalid ? k_is : -1;
 #pragma unroll
             for (int o = kLanesPerRow; o < 32; o <<= 1) {
@@ -427,6 +465,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           __syncwarp();
         }
+      }
+      if (xq_n > 0) {
+        evaluated += exact_queue_flush(R, d, s_xq[warp], xq_n, lane);
+        __syncwarp();
       }
     }
     __syncthreads();

@@ -44,7 +44,6 @@ namespace {
 using wrt::Arena;
 using Clock = std::chrono::steady_clock;
 
-constexpr size_t kAlign = Arena::kAlign;
 size_t al(size_t b) { return Arena::round_up(b); }
 
 // Device tables of one sphere-grid shape, in one arena block.

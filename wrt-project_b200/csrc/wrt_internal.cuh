@@ -123,6 +123,16 @@ struct StagedConfig {
 extern const StagedConfig kStagedConfigs[];
 extern const int kNumStagedConfigs;
 int staged_smem_bytes(int n, int *tile_h, int *qpitch);
+// Guard band (in cells) of the staged kernel's x / y cell fractions.  Its
+// FP32 cell coordinate q = fma(j, du, q0) has q0 and du rounded once from
+// FP64, so |q - q_exact| <= 0.5 ulp(q0) + |j| |du| 2^-24 + 0.5 ulp(q) with
+// |q0| < 1.4 n, |du| < 1/2, |j| <= L: below 1.4e-7 n + 3e-8 L.  The band is
+// twice that, so every sample whose exact coordinate is on a cell boundary
+// (where the reference's cell index and fraction can disagree) or on a cube
+// face lies inside it.
+inline float staged_guard(int n, int L) {
+  return 3.0e-7f * (float)(n > 32 ? n : 32) + 6.0e-8f * (float)L;
+}
 constexpr int kStagedDirChunk = 512;  // directions per work item
 constexpr int kStagedSmemMax = 200 * 1024;  // staged tile budget (bytes of shared memory)
 int plane_staged_launch(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
@@ -286,6 +296,23 @@ __device__ __forceinline__ float ldv(const float *v, int n, int ix, int iy, int 
   return __ldg(v + ((size_t)ix * n + iy) * n + iz);
 }
 
+// fmod(x, y) for x >= 0, y > 0 and x / y < 2^52: the exact remainder x - n y,
+// n = trunc(x / y).  The quotient estimate from the rounded division is off
+// by at most one; a single fused multiply-add then gives x - n y exactly
+// (the true remainder is representable), so the result equals fmod's.
+__device__ __forceinline__ double exact_rem(double x, double y) {
+  double n = trunc(__ddiv_rn(x, y));
+  double r = fma(-n, y, x);
+  if (r < 0.0) {
+    n -= 1.0;
+    r = fma(-n, y, x);
+  } else if (r >= y) {
+    n += 1.0;
+    r = fma(-n, y, x);
+  }
+  return r;
+}
+
 // cube_trilinear_interp, radon_grid/src/interp.c:25-60.
 static __device__ __noinline__ double exact_trilinear(const float *v, int n, double x, double y,
                                                double z) {
@@ -294,8 +321,8 @@ static __device__ __noinline__ double exact_trilinear(const float *v, int n, dou
   const double x1 = __dadd_rn(x, 1.0), y1 = __dadd_rn(y, 1.0), z1 = __dadd_rn(z, 1.0);
   int ix = (int)__ddiv_rn(x1, delta), iy = (int)__ddiv_rn(y1, delta),
       iz = (int)__ddiv_rn(z1, delta);
-  double cx = __ddiv_rn(fmod(x1, delta), delta), cy = __ddiv_rn(fmod(y1, delta), delta),
-         cz = __ddiv_rn(fmod(z1, delta), delta);
+  double cx = __ddiv_rn(exact_rem(x1, delta), delta), cy = __ddiv_rn(exact_rem(y1, delta), delta),
+         cz = __ddiv_rn(exact_rem(z1, delta), delta);
   if (ix == n - 1) { ix -= 1; cx = 1.0; }
   if (iy == n - 1) { iy -= 1; cy = 1.0; }
   if (iz == n - 1) { iz -= 1; cz = 1.0; }
