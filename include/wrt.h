@@ -152,8 +152,20 @@ int wrt_radon_transpose(wrt_ctx *ctx, const double *g, int ngrid, int nphi, int 
                         int nshift, const wrt_plane_opts *opts, double *out_volume);
 
 /* ------------------------------------------------ device-resident objects */
+typedef enum wrt_storage {
+  WRT_STORAGE_F32 = 0, /* FP32 node values (default) */
+  WRT_STORAGE_BF16 = 1 /* bfloat16 node values, FP32 arithmetic: half the device memory */
+} wrt_storage;
+
 /* A volume held on the device in the layouts the kernels read. */
 int wrt_volume_create(wrt_ctx *ctx, int ngrid, wrt_volume **out);
+/* The same with a storage precision (wrt_storage).  A BF16 volume rounds each
+ * value to bfloat16 (nearest even) on upload; the trilinear sampler of the
+ * staged kernel (single, batched) interpolates the rounded values in FP32,
+ * the guard-band samples in FP64.  No counterpart in the reference (FP64). */
+int wrt_volume_create_storage(wrt_ctx *ctx, int ngrid, int storage, wrt_volume **out);
+/* Device bytes the volume holds (values, layer pairs once built, statistics). */
+size_t wrt_volume_bytes(const wrt_volume *vol);
 /* Upload from host memory (exactly one of f64 / f32 non-NULL), ordered on
  * the context's stream.  Pinned host memory makes the copy asynchronous. */
 int wrt_volume_upload(wrt_volume *vol, const double *host_f64, const float *host_f32);

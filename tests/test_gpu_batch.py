@@ -95,3 +95,52 @@ def test_batch_rejects_bad_requests(ctx):
     with pytest.raises(wrt.WrtError):
         wrt.radon_forward_batch(ctx, [(v, g, 0, 0)])
     wrt.radon_forward_batch(ctx, [])  # empty batch: nothing to do
+
+
+# ----------------------------------------------------------- BF16 storage
+def test_bf16_volume_matches_oracle_on_rounded_values(ctx):
+    n, grid, L = 40, (12, 6, 14), 40
+    vol = ellipsoid_phantom(n, 8, 4040)
+    v16 = wrt.Volume(ctx, n, storage=wrt.STORAGE_BF16)
+    v16.upload(vol)
+    v32 = wrt.Volume(ctx, n)
+    v32.upload(vol)
+    g = wrt.Grid(ctx, *grid)
+    out = wrt.DeviceBuffer(ctx, g.nplanes * 8)
+    shape = (grid[2], grid[0], grid[1])
+    wrt.radon_forward_device(ctx, v16, g, out.ptr, sampler=wrt.TRILINEAR, half_extent=L)
+    got16 = out.download(np.empty(shape))
+    # exact parity with the FP64 oracle on the values the volume holds
+    ref16 = O.radon_forward(wrt.round_bf16(vol), *grid, sampler=O.TRILINEAR, half_extent=L)
+    assert rel_l2(got16, ref16) < TOL_L2
+    assert rel_max(got16, ref16) < 1e-4
+    # against the unrounded volume the error is the storage rounding (bf16: 8 bits)
+    ref = O.radon_forward(vol, *grid, sampler=O.TRILINEAR, half_extent=L)
+    assert rel_l2(got16, ref) < 4e-3
+    # half the device memory of the FP32 layouts, once the layer pairs exist
+    wrt.radon_forward_device(ctx, v32, g, out.ptr, sampler=wrt.TRILINEAR, half_extent=L)
+    assert v16.nbytes * 2 <= v32.nbytes + 64
+    # BF16 volumes are sampled by the staged kernel only
+    with pytest.raises(wrt.WrtError):
+        wrt.radon_forward_device(ctx, v16, g, out.ptr, sampler=wrt.NEAREST)
+
+
+def test_batch_mixes_fp32_and_bf16_volumes(ctx):
+    reqs, outs = [], []
+    for k, (n, storage) in enumerate([(24, wrt.STORAGE_F32), (30, wrt.STORAGE_BF16),
+                                       (36, wrt.STORAGE_BF16)]):
+        vol = ellipsoid_phantom(n, 5, 60 + k)
+        v = wrt.Volume(ctx, n, storage=storage)
+        v.upload(vol)
+        g = wrt.Grid(ctx, 8, 4, 9)
+        out = wrt.DeviceBuffer(ctx, g.nplanes * 8)
+        reqs.append((v, g, out.ptr, n))
+        outs.append((vol, storage, out))
+    wrt.radon_forward_batch(ctx, reqs)
+    ctx.synchronize()
+    for vol, storage, out in outs:
+        got = out.download(np.empty((9, 8, 4)))
+        held = wrt.round_bf16(vol) if storage == wrt.STORAGE_BF16 else vol.astype(np.float32)
+        ref = O.radon_forward(held.astype(np.float64), 8, 4, 9, sampler=O.TRILINEAR,
+                              half_extent=vol.shape[0])
+        assert rel_l2(got, ref) < TOL_L2

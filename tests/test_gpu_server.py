@@ -153,18 +153,17 @@ def test_request_larger_than_budget_is_refused():
 
 
 def test_requests_arriving_during_a_launch_overlap_it():
-    rng = np.random.default_rng(77)
-    big = ellipsoid_phantom(96, 8, 1).astype(np.float32)
+    big = ellipsoid_phantom(128, 8, 1).astype(np.float32)
+    small = [ellipsoid_phantom(24, 4, 300 + k).astype(np.float32) for k in range(6)]
+    outs = [np.zeros((8, 8, 4)) for _ in small]
     with wrt.Server(0, budget_bytes=1 << 30, max_batch=8, max_inflight=2) as srv:
-        out0 = np.zeros((64, 32, 16))
-        first = srv.submit_forward(big, 32, 16, 64, out0, half_extent=96)
-        later = []
-        for k in range(6):
-            vol = ellipsoid_phantom(24, 4, 300 + k).astype(np.float32)
-            out = np.zeros((8, 8, 4))
-            later.append(srv.submit_forward(vol, 8, 4, 8, out, half_extent=24))
+        out0 = np.zeros((128, 64, 32))
+        first = srv.submit_forward(big, 64, 32, 128, out0, half_extent=128)
+        # submitted microseconds later, while the first launch runs
+        later = [srv.submit_forward(v, 8, 4, 8, o, half_extent=24) for v, o in zip(small, outs)]
         i0 = srv.wait(first, WAIT_MS)
         infos = [srv.wait(i, WAIT_MS) for i in later]
     assert i0.status == 0 and all(i.status == 0 for i in infos)
-    # the later requests were launched before the first one finished
+    # the later requests were admitted and launched before the first one finished
     assert min(i.start_ms for i in infos) < i0.done_ms
+    assert max(i.batch_size for i in infos) > 1

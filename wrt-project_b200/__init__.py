@@ -27,6 +27,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "lib" / "libwrt.so"
 
 NEAREST, TRILINEAR = 0, 1
+STORAGE_F32, STORAGE_BF16 = 0, 1
 KERNEL_AUTO, KERNEL_PLAIN, KERNEL_STAGED = 0, 1, 2
 
 STATUS = {
@@ -114,6 +115,9 @@ def lib() -> C.CDLL:
         L.wrt_radon3d_adjoint.argtypes = [_vp, _dp, _i, _i, _i, _i, _dp]
         L.wrt_radon_transpose.argtypes = [_vp, _dp, _i, _i, _i, _i, C.POINTER(PlaneOpts), _dp]
         L.wrt_volume_create.argtypes = [_vp, _i, C.POINTER(_vp)]
+        L.wrt_volume_create_storage.argtypes = [_vp, _i, _i, C.POINTER(_vp)]
+        L.wrt_volume_bytes.argtypes = [_vp]
+        L.wrt_volume_bytes.restype = _sz
         L.wrt_volume_upload.argtypes = [_vp, _vp, _vp]
         L.wrt_volume_upload_device.argtypes = [_vp, _vp]
         L.wrt_volume_destroy.argtypes = [_vp]
@@ -347,11 +351,18 @@ class PinnedArray:
 
 
 class Volume:
-    """A volume resident on the device (wrt_volume)."""
+    """A volume resident on the device (wrt_volume); storage STORAGE_F32 or
+    STORAGE_BF16 (values rounded to bfloat16, half the device memory)."""
 
-    def __init__(self, ctx: Context, n: int):
+    def __init__(self, ctx: Context, n: int, storage: int = STORAGE_F32):
         self.ctx, self.n, self._h = ctx, int(n), _vp()
-        ctx.check(lib().wrt_volume_create(ctx.handle, self.n, C.byref(self._h)), "volume_create")
+        self.storage = int(storage)
+        ctx.check(lib().wrt_volume_create_storage(ctx.handle, self.n, self.storage,
+                                                  C.byref(self._h)), "volume_create")
+
+    @property
+    def nbytes(self) -> int:
+        return int(lib().wrt_volume_bytes(self._h))
 
     @property
     def handle(self):
@@ -529,3 +540,12 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def round_bf16(a) -> np.ndarray:
+    """Values rounded to bfloat16 (round to nearest even), as float64: what a
+    STORAGE_BF16 volume holds."""
+    x = np.ascontiguousarray(a, dtype=np.float32)
+    b = x.view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)

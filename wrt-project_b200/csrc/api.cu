@@ -27,6 +27,9 @@ struct wrt_volume {
   int pitch = 0;
   size_t vol_bytes = 0, pair_bytes = 0;
   bool pairs_valid = false;
+  int storage = WRT_STORAGE_F32;        // BF16: d_vol16 / d_pairs16 replace d_vol / d_pairs
+  __nv_bfloat16 *d_vol16 = nullptr;     // n^3 bf16 values, v[ix][iy][iz]
+  __nv_bfloat162 *d_pairs16 = nullptr;  // layer pairs as bf16x2
 };
 
 struct wrt_grid {
@@ -345,7 +348,12 @@ int wrt_radon_grid_init(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *
 
 // ------------------------------------------------------------ resident objects
 int wrt_volume_create(wrt_ctx *ctx, int n, wrt_volume **out) {
+  return wrt_volume_create_storage(ctx, n, WRT_STORAGE_F32, out);
+}
+
+int wrt_volume_create_storage(wrt_ctx *ctx, int n, int storage, wrt_volume **out) {
   if (!ctx || !out || n < 2 || n > 2048) return WRT_ERR_INVALID_ARGUMENT;
+  if (storage != WRT_STORAGE_F32 && storage != WRT_STORAGE_BF16) return WRT_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   int st = set_device(ctx);
   if (st) return st;
@@ -353,8 +361,15 @@ int wrt_volume_create(wrt_ctx *ctx, int n, wrt_volume **out) {
   if (!v) return WRT_ERR_OUT_OF_MEMORY;
   v->ctx = ctx;
   v->n = n;
-  v->vol_bytes = sizeof(float) * (size_t)n * n * n;
-  st = ctx_alloc(ctx, (void **)&v->d_vol, v->vol_bytes);
+  v->storage = storage;
+  const size_t count = (size_t)n * n * n;
+  if (storage == WRT_STORAGE_BF16) {
+    v->vol_bytes = sizeof(__nv_bfloat16) * count;
+    st = ctx_alloc(ctx, (void **)&v->d_vol16, v->vol_bytes);
+  } else {
+    v->vol_bytes = sizeof(float) * count;
+    st = ctx_alloc(ctx, (void **)&v->d_vol, v->vol_bytes);
+  }
   if (!st) st = ctx_alloc(ctx, (void **)&v->d_stats, 2 * sizeof(unsigned int));
   if (st) {
     wrt_volume_destroy(v);
@@ -380,13 +395,17 @@ int volume_finish_upload(wrt_volume *v) {
 int volume_ensure_pairs(wrt_volume *v) {
   if (v->pairs_valid) return WRT_OK;
   wrt_ctx *ctx = v->ctx;
-  if (!v->d_pairs) {
+  const bool bf16 = v->storage == WRT_STORAGE_BF16;
+  if (!v->d_pairs && !v->d_pairs16) {
     v->pitch = v->n + (v->n & 1);
-    v->pair_bytes = sizeof(float2) * (size_t)(v->n - 1) * v->n * v->pitch;
-    int st = ctx_alloc(ctx, (void **)&v->d_pairs, v->pair_bytes);
+    v->pair_bytes = (bf16 ? sizeof(__nv_bfloat162) : sizeof(float2)) * (size_t)(v->n - 1) * v->n *
+                    v->pitch;
+    int st = bf16 ? ctx_alloc(ctx, (void **)&v->d_pairs16, v->pair_bytes)
+                  : ctx_alloc(ctx, (void **)&v->d_pairs, v->pair_bytes);
     if (st) return st;
   }
-  int st = volume_pairs(ctx, v->d_vol, v->n, v->d_pairs, v->pitch);
+  int st = bf16 ? volume_pairs_bf16(ctx, v->d_vol16, v->n, v->d_pairs16, v->pitch)
+                : volume_pairs(ctx, v->d_vol, v->n, v->d_pairs, v->pitch);
   if (!st) v->pairs_valid = true;
   return st;
 }
@@ -398,12 +417,16 @@ int wrt_volume_upload(wrt_volume *v, const double *f64, const float *f32) {
   int st = set_device(ctx);
   if (st) return st;
   const size_t count = (size_t)v->n * v->n * v->n;
-  DevBuf stage(ctx);
+  const bool bf16 = v->storage == WRT_STORAGE_BF16;
+  DevBuf stage(ctx), vol32(ctx);
   st = stage.alloc(count * (f64 ? sizeof(double) : sizeof(float)));
+  if (!st && bf16) st = vol32.alloc(count * sizeof(float));
+  float *dst = bf16 ? vol32.as<float>() : v->d_vol;
   if (!st) st = h2d(ctx, stage.p, f64 ? (const void *)f64 : (const void *)f32, stage.bytes, "volume upload");
   if (!st)
-    st = f64 ? volume_from_f64(ctx, stage.as<double>(), v->n, v->d_vol, v->d_stats)
-             : volume_from_f32(ctx, stage.as<float>(), v->n, v->d_vol, v->d_stats);
+    st = f64 ? volume_from_f64(ctx, stage.as<double>(), v->n, dst, v->d_stats)
+             : volume_from_f32(ctx, stage.as<float>(), v->n, dst, v->d_stats);
+  if (!st && bf16) st = volume_to_bf16(ctx, dst, v->n, v->d_vol16, v->d_stats);
   if (!st) st = volume_finish_upload(v);  // also keeps the staging buffer alive until done
   return st;
 }
@@ -412,9 +435,14 @@ int wrt_volume_upload_device(wrt_volume *v, const float *dev_f32) {
   if (!v || !dev_f32) return WRT_ERR_INVALID_ARGUMENT;
   int st = set_device(v->ctx);
   if (st) return st;
-  st = volume_from_f32(v->ctx, dev_f32, v->n, v->d_vol, v->d_stats);
+  st = v->storage == WRT_STORAGE_BF16 ? volume_to_bf16(v->ctx, dev_f32, v->n, v->d_vol16, v->d_stats)
+                                      : volume_from_f32(v->ctx, dev_f32, v->n, v->d_vol, v->d_stats);
   if (!st) st = volume_finish_upload(v);
   return st;
+}
+
+size_t wrt_volume_bytes(const wrt_volume *v) {
+  return v ? v->vol_bytes + v->pair_bytes + 2 * sizeof(unsigned int) : 0;
 }
 
 int wrt_volume_destroy(wrt_volume *v) {
@@ -423,8 +451,10 @@ int wrt_volume_destroy(wrt_volume *v) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx_free(ctx, v->d_vol, v->vol_bytes);
+  ctx_free(ctx, v->d_vol16, v->vol_bytes);
   ctx_free(ctx, v->d_stats, 2 * sizeof(unsigned int));
   ctx_free(ctx, v->d_pairs, v->pair_bytes);
+  ctx_free(ctx, v->d_pairs16, v->pair_bytes);
   delete v;
   return WRT_OK;
 }
@@ -500,8 +530,10 @@ int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, in
   int th = 0, qp = 0;
   const int smem = staged_smem_bytes(n, &th, &qp);
   StagedReq r = {};
-  r.pairs = vol->d_pairs;
-  r.vol = vol->d_vol;
+  const bool bf16 = vol->storage == WRT_STORAGE_BF16;
+  r.pairs = bf16 ? (const void *)vol->d_pairs16 : (const void *)vol->d_pairs;
+  r.vol = bf16 ? (const void *)vol->d_vol16 : (const void *)vol->d_vol;
+  r.storage = vol->storage;
   r.dir = grid->d_dir;
   r.dir32 = grid->d_dir32;
   r.shift = grid->d_shift;
@@ -557,6 +589,9 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const wrt_gri
                          staged_smem_bytes(vol->n, &th, &qp) > 0;
   if (o.kernel == WRT_KERNEL_STAGED && !staged_ok)
     return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "staged kernel needs the trilinear sampler");
+  if (vol->storage == WRT_STORAGE_BF16 && (o.kernel == WRT_KERNEL_PLAIN || !staged_ok))
+    return fail(ctx, WRT_ERR_INVALID_ARGUMENT,
+                "BF16 volumes are sampled by the staged kernel (trilinear sampler) only");
   if (o.kernel != WRT_KERNEL_PLAIN && staged_ok) return radon_forward_staged(ctx, vol, grid, L, dev_out);
   PlaneJob job = {};
   job.vol = vol->d_vol;
@@ -597,9 +632,11 @@ int wrt_radon_forward_batch(wrt_ctx *ctx, const wrt_forward_req *reqs, int nreq)
     if (st) return st;
     const int L = reqs[r].half_extent ? reqs[r].half_extent : 2 * n;
     StagedReq q;
-    staged_request(n, vol->pitch, grid->nphi * grid->ntheta, grid->nshift, L, vol->d_pairs,
-                   vol->d_vol, grid->d_dir, grid->d_dir32, grid->d_shift, grid->d_shift32,
-                   reqs[r].dev_out, &q);
+    const bool bf16 = vol->storage == WRT_STORAGE_BF16;
+    staged_request(n, vol->pitch, grid->nphi * grid->ntheta, grid->nshift, L, vol->storage,
+                   bf16 ? (const void *)vol->d_pairs16 : (const void *)vol->d_pairs,
+                   bf16 ? (const void *)vol->d_vol16 : (const void *)vol->d_vol, grid->d_dir,
+                   grid->d_dir32, grid->d_shift, grid->d_shift32, reqs[r].dev_out, &q);
     FwdAux a = {};
     a.vol = vol->d_vol;
     a.pairs = vol->d_pairs;

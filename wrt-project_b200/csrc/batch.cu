@@ -176,8 +176,8 @@ constexpr int kBatchKernels = 7;  // kernels per graph launch
 
 namespace wrt {
 
-void staged_request(int n, int pitch, int ndir, int nshift, int L, const float2 *pairs,
-                    const float *vol, const double *dir, const float *dir32,
+void staged_request(int n, int pitch, int ndir, int nshift, int L, int storage,
+                    const void *pairs, const void *vol, const double *dir, const float *dir32,
                     const double *shift, const float *shift32, double *out, StagedReq *r) {
   int th = 0, qp = 0;
   staged_smem_bytes(n, &th, &qp);
@@ -196,6 +196,7 @@ void staged_request(int n, int pitch, int ndir, int nshift, int L, const float2 
   r->ndir = ndir;
   r->nshift = nshift;
   r->L = L;
+  r->storage = storage;
   r->guard = staged_guard(n, L);
   r->crop_r2 = 3.0f + 1e-5f;
   r->scale = 1.0;

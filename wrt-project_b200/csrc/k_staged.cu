@@ -86,6 +86,13 @@ __device__ __forceinline__ u64 sub2(u64 a, u64 b) {
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
+// FP64 scalar from shared memory, re-read at every use (keeps row-geometry
+// constants out of the registers the sample loop needs)
+__device__ __forceinline__ double ldsd(const double *p) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
+  return v;
+}
 // 16-byte shared-memory load as two pairs, 32-bit shared address
 __device__ __forceinline__ void lds_pairs(unsigned addr, u64 &lo, u64 &hi) {
   asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(lo), "=l"(hi) : "r"(addr));
@@ -141,10 +148,6 @@ __device__ __forceinline__ bool clip_lin(float q0, float dq, float inv, float lo
   return jlo <= jhi;
 }
 
-struct Dir64 {
-  double nx, ny, nz, a1x, a1y, a1z;  // normal and delta * v1
-};
-
 __device__ __noinline__ double exact_sample(const wrt::StagedReq &R, int d, int is, int i, int j) {
   const double *D = R.dir + 9 * (size_t)d;
   const double s = R.shift[is];
@@ -156,7 +159,9 @@ __device__ __noinline__ double exact_sample(const wrt::StagedReq &R, int d, int 
                               __dmul_rn(__dmul_rn(delta, D[7]), dj));
   const double pz = __dadd_rn(__dadd_rn(__dmul_rn(s, D[2]), __dmul_rn(__dmul_rn(delta, D[5]), di)),
                               __dmul_rn(__dmul_rn(delta, D[8]), dj));
-  return wrtd::exact_trilinear(R.vol, R.n, px, py, pz);
+  return R.storage == WRT_STORAGE_BF16
+             ? wrtd::exact_trilinear(static_cast<const __nv_bfloat16 *>(R.vol), R.n, px, py, pz)
+             : wrtd::exact_trilinear(static_cast<const float *>(R.vol), R.n, px, py, pz);
 }
 
 // Sample classification shared by the fast walk and the guard-band walk (the
@@ -207,6 +212,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ unsigned char s_rowlane[kWarps][32];  // compacted non-empty rows -> lane
   // guard-band samples waiting for the FP64 path: (shift index, i << 16 | j)
   __shared__ int2 s_xq[kWarps][64];
+  // FP64 row geometry: per item (h, 1/h, layer bounds) and per warp's direction
+  // (normal, delta v1, 1/(delta v1z))
+  __shared__ double s_item_geo[4];
+  __shared__ double s_dir_geo[kWarps][8];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int pos = lane % kLanesPerRow;  // position of this lane within its row
   const unsigned smem0 = (unsigned)__cvta_generic_to_shared(quads);
@@ -228,17 +237,31 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int qp = R.qpitch;
     const int y0 = item.tile * R.tile_h;
     const int H = min(R.tile_h, W - y0);
+    // layer bounds of the row enumeration; rows within kZBand of a node layer
+    // (or of the cube's z faces) are evaluated exactly (visible to all warps
+    // after the staging barrier below)
+    if (tid == 0) {
+      const double h64 = 0.5 * (double)W;
+      s_item_geo[0] = h64;
+      s_item_geo[1] = 1.0 / h64;
+      s_item_geo[2] = item.layer == 0 ? -kZBand : (double)item.layer;
+      s_item_geo[3] = item.layer == W - 1 ? (double)W + kZBand : (double)(item.layer + 1);
+    }
     // ---- stage layer pair (iz, iz+1), node rows y0 .. y0+H, cells -2 .. W+1
     {
-      const float2 *src = R.pairs + (size_t)item.layer * n * R.pitch2 + (size_t)y0 * R.pitch2;
+      const size_t base = (size_t)item.layer * n * R.pitch2 + (size_t)y0 * R.pitch2;
+      const float2 *src = static_cast<const float2 *>(R.pairs) + base;
+      const __nv_bfloat162 *src16 = static_cast<const __nv_bfloat162 *>(R.pairs) + base;
+      const bool bf16 = R.storage == WRT_STORAGE_BF16;
       const int wide = W + 2 * kPadX;
       const int total = (H + 1) * wide;
       for (int k = tid; k < total; k += kThreads) {
         const int yy = k / wide, xc = k - yy * wide, x = xc - kPadX;
         float4 q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (x >= 0 && x < W) {
-          const float2 *row = src + (size_t)yy * R.pitch2;
-          const float2 a = __ldg(row + x), b = __ldg(row + x + 1);
+          const size_t o = (size_t)yy * R.pitch2 + x;
+          const float2 a = bf16 ? __bfloat1622float2(__ldg(src16 + o)) : __ldg(src + o);
+          const float2 b = bf16 ? __bfloat1622float2(__ldg(src16 + o + 1)) : __ldg(src + o + 1);
           const float dz0 = a.y - a.x, dz1 = b.y - b.x;
           q = make_float4(a.x, b.x - a.x, dz0, dz1 - dz0);
         }
@@ -249,11 +272,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     const float delta = 1.0f / (float)n;
     const float g = R.guard;
     const float halfband = 0.5f - g;
-    // layer bounds of the row enumeration; rows within kZBand of a node layer
-    // (or of the cube's z faces) are evaluated exactly
-    const double h64 = 0.5 * (double)W, inv_h64 = 1.0 / h64, delta64 = 1.0 / (double)n;
-    const double wlo = item.layer == 0 ? -kZBand : (double)item.layer;
-    const double whi = item.layer == W - 1 ? (double)W + kZBand : (double)(item.layer + 1);
     const float rc2 = R.crop_r2;
     const int L = R.L;
     // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x + magic))
@@ -267,17 +285,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (dl >= item.ndir) break;
       const int d = item.dir0 + dl;
       const double *Dd = R.dir + 9 * (size_t)d;
-      Dir64 D;
-      D.nx = __ldg(Dd + 0);
-      D.ny = __ldg(Dd + 1);
-      D.nz = __ldg(Dd + 2);
-      D.a1x = __ldg(Dd + 3) * delta64;
-      D.a1y = __ldg(Dd + 4) * delta64;
-      D.a1z = __ldg(Dd + 5) * delta64;
-      const double inv_a1z = D.a1z != 0.0 ? 1.0 / D.a1z : 0.0;
+      double *G = s_dir_geo[warp];
+      {
+        const double delta64 = 1.0 / (double)n;
+        if (lane < 6) G[lane] = __ldg(Dd + lane) * (lane >= 3 ? delta64 : 1.0);
+        if (lane == 6) G[6] = 1.0 / (__ldg(Dd + 5) * delta64);
+        __syncwarp();
+      }
       // per-sample steps in cell units, rounded once to FP32
-      const float du = (float)(__ldg(Dd + 6) * delta64 * h64);
-      const float dv = (float)(__ldg(Dd + 7) * delta64 * h64);
+      const float du = (float)(__ldg(Dd + 6) * (1.0 / (double)n) * ldsd(&s_item_geo[0]));
+      const float dv = (float)(__ldg(Dd + 7) * (1.0 / (double)n) * ldsd(&s_item_geo[0]));
       const float inv_du = du != 0.0f ? 1.0f / du : 0.0f;
       const float inv_dv = dv != 0.0f ? 1.0f / dv : 0.0f;
       const u64 duv = pk2(du, dv);
@@ -296,8 +313,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             const float rem = rc2 - s * s;
             if (rem >= 0.0f) {
               const int im = (int)floorf(sqrtf(rem) / delta) + 1;
-              cnt[k] = rows_in_layer(__ldg(R.shift + is), D.nz, D.a1z, inv_a1z, h64, inv_h64, wlo,
-                                     whi, max(-L, -im), min(L - 1, im), &ia[k]);
+              cnt[k] = rows_in_layer(__ldg(R.shift + is), ldsd(G + 2), ldsd(G + 5), ldsd(G + 6),
+                                     ldsd(&s_item_geo[0]), ldsd(&s_item_geo[1]),
+                                     ldsd(&s_item_geo[2]), ldsd(&s_item_geo[3]), max(-L, -im),
+                                     min(L - 1, im), &ia[k]);
             }
           }
           lane_total += cnt[k];
@@ -341,12 +360,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             const float s = __ldg(R.shift32 + is);
             const double s64 = __ldg(R.shift + is), di64 = (double)i;
             const float di = (float)i;
-            const double tz64 = row_w(s64, D.nz, D.a1z, di64, h64) - (double)item.layer;
+            const double h64 = ldsd(&s_item_geo[0]);
+            const double tz64 = row_w(s64, ldsd(G + 2), ldsd(G + 5), di64, h64) - (double)item.layer;
             tz = (float)tz64;
             zexact = tz64 < kZBand || tz64 > 1.0 - kZBand;
-            // row origin in cell units, FP64 then rounded once (minus 1/2 applied below)
-            ub = (float)((fma(di64, D.a1x, s64 * D.nx) + 1.0) * h64 - 0.5);
-            vb = (float)((fma(di64, D.a1y, s64 * D.ny) + 1.0) * h64 - 0.5);
+            // row origin in cell units (q - 1/2 at j = 0), FP64 then rounded once
+            ub = (float)((fma(di64, ldsd(G + 3), s64 * ldsd(G + 0)) + 1.0) * h64 - 0.5);
+            vb = (float)((fma(di64, ldsd(G + 4), s64 * ldsd(G + 1)) + 1.0) * h64 - 0.5);
             const float rem = rc2 - s * s - (delta * di) * (delta * di);
             if (rem >= 0.0f) {
               const int jm = (int)floorf(sqrtf(rem) / delta) + 1;
@@ -437,7 +457,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                   xq_n += __popc(m);
                   __syncwarp();
                   if (xq_n >= 32) {
-                    evaluated += exact_queue_flush(R, d, s_xq[warp], 32, lane);
+                    const int ev = exact_queue_flush(R, d, s_xq[warp], 32, lane);
+                    if (kCount) evaluated += ev;
                     if (lane < xq_n - 32) s_xq[warp][lane] = s_xq[warp][lane + 32];
                     xq_n -= 32;
                     __syncwarp();
@@ -467,7 +488,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
       if (xq_n > 0) {
-        evaluated += exact_queue_flush(R, d, s_xq[warp], xq_n, lane);
+        const int ev = exact_queue_flush(R, d, s_xq[warp], xq_n, lane);
+        if (kCount) evaluated += ev;
         __syncwarp();
       }
     }

@@ -61,6 +61,48 @@ __global__ void volume_pairs_kernel(const float *__restrict__ v, int n, float2 *
   }
 }
 
+// BF16 storage: each value rounded to bfloat16; statistics of the rounded values.
+__global__ void volume_bf16_kernel(const float *__restrict__ src, int n,
+                                   __nv_bfloat16 *__restrict__ dst, unsigned int *__restrict__ stats) {
+  const size_t total = (size_t)n * n * n;
+  float local = 0.0f, amax = 0.0f;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const __nv_bfloat16 b = __float2bfloat16_rn(src[k]);
+    dst[k] = b;
+    const float v = __bfloat162float(b);
+    amax = fmaxf(amax, fabsf(v));
+    if (v != 0.0f) {
+      const int iz = (int)(k % n), iy = (int)((k / n) % n), ix = (int)(k / ((size_t)n * n));
+      local = fmaxf(local, wrtd::node_r2(ix, iy, iz, n));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    local = fmaxf(local, __shfl_xor_sync(0xffffffffu, local, o));
+    amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (local > 0.0f) atomicMax(stats, __float_as_uint(local));
+    if (amax > 0.0f) atomicMax(stats + 1, __float_as_uint(amax));
+  }
+}
+
+__global__ void volume_pairs_bf16_kernel(const __nv_bfloat16 *__restrict__ v, int n,
+                                         __nv_bfloat162 *__restrict__ pairs, int pitch) {
+  const size_t total = (size_t)(n - 1) * n * pitch;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    int ix = (int)(k % pitch), iy = (int)((k / pitch) % n), iz = (int)(k / ((size_t)pitch * n));
+    __nv_bfloat162 p = __floats2bfloat162_rn(0.0f, 0.0f);
+    if (ix < n) {
+      const __nv_bfloat16 *q = v + ((size_t)ix * n + iy) * n + iz;
+      p.x = q[0];
+      p.y = q[1];
+    }
+    pairs[k] = p;
+  }
+}
+
 template <typename T>
 int convert(wrt_ctx *ctx, const T *d_src, int n, float *d_vol, unsigned int *d_stats) {
   cudaError_t e = cudaMemsetAsync(d_stats, 0, 2 * sizeof(unsigned int), ctx->stream);
@@ -83,6 +125,22 @@ int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
 int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
                     unsigned int *d_r2bits) {
   return convert(ctx, d_src, n, d_vol, d_r2bits);
+}
+
+int volume_to_bf16(wrt_ctx *ctx, const float *d_vol, int n, __nv_bfloat16 *d_vol16,
+                   unsigned int *d_stats) {
+  cudaError_t e = cudaMemsetAsync(d_stats, 0, 2 * sizeof(unsigned int), ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "volume stats reset");
+  volume_bf16_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(d_vol, n, d_vol16, d_stats);
+  ctx->launches++;
+  return check_launch(ctx, "volume_bf16_kernel");
+}
+
+int volume_pairs_bf16(wrt_ctx *ctx, const __nv_bfloat16 *d_vol16, int n,
+                      __nv_bfloat162 *d_pairs, int pitch) {
+  volume_pairs_bf16_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(d_vol16, n, d_pairs, pitch);
+  ctx->launches++;
+  return check_launch(ctx, "volume_pairs_bf16_kernel");
 }
 
 int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch) {

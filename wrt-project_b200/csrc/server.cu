@@ -306,8 +306,8 @@ void add_to_batch(wrt_server *s, Request *q, wrt::BatchBuilder &b) {
         base + al(4 * nn * nn * nn) + al(8 * (nn - 1) * nn * forward_pitch(n)));
     const int L = r.half_extent ? r.half_extent : 2 * n;
     wrt::StagedReq sr;
-    wrt::staged_request(n, (int)forward_pitch(n), ndir, r.nshift, L, pairs, vol, g->dir,
-                        g->dir32, g->shift, g->shift32, q->d_out, &sr);
+    wrt::staged_request(n, (int)forward_pitch(n), ndir, r.nshift, L, WRT_STORAGE_F32, pairs,
+                        vol, g->dir, g->dir32, g->shift, g->shift32, q->d_out, &sr);
     wrt::FwdAux a = {};
     a.vol = vol;
     a.pairs = pairs;

@@ -20,6 +20,7 @@
 // and the trilinear value is continuous, so the FP32 result differs from the
 // reference only by rounding.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -82,6 +83,12 @@ int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
 int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
                     unsigned int *d_stats);
 int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch);
+// BF16 storage: values rounded to bfloat16 (nearest even); statistics of the
+// rounded values; layer pairs as bf16x2.
+int volume_to_bf16(wrt_ctx *ctx, const float *d_vol, int n, __nv_bfloat16 *d_vol16,
+                   unsigned int *d_stats);
+int volume_pairs_bf16(wrt_ctx *ctx, const __nv_bfloat16 *d_vol16, int n,
+                      __nv_bfloat162 *d_pairs, int pitch);
 
 // Plane kernels (k_plane.cu).
 struct PlaneJob {
@@ -103,14 +110,15 @@ int plane_transpose(wrt_ctx *ctx, const PlaneJob &job, const double *d_g, double
 
 // Staged plane kernel (k_staged.cu).
 struct StagedReq {
-  const float2 *pairs;     // layer pairs [iz][y][pitch2]
-  const float *vol;        // reference layout, for guard-band samples
+  const void *pairs;       // layer pairs [iz][y][pitch2]: float2 (FP32) or bf16x2 (BF16 storage)
+  const void *vol;         // reference layout, for guard-band samples: float or bf16
   const double *dir;       // [ndir][9] FP64 directions
   const float *dir32;      // [ndir][8]: normal, v1, v2.x, v2.y (unscaled) FP32
   const double *shift;     // [nshift]
   const float *shift32;    // [nshift]
   unsigned long long *acc; // [nshift][ndir] fixed-point accumulators (the output buffer)
-  int n, pitch2, qpitch, tile_h, ndir, nshift, L, pad;
+  int n, pitch2, qpitch, tile_h, ndir, nshift, L;
+  int storage;             // wrt_storage of pairs / vol
   float guard, crop_r2;
   double scale;            // fixed-point scale 2^k
 };
@@ -221,8 +229,8 @@ int batch_slot_init(wrt_ctx *ctx, BatchSlot *slot, cudaStream_t stream);
 int batch_slot_launch(BatchSlot *slot, BatchBuilder &b);
 void batch_slot_release(BatchSlot *slot);
 // Fills a StagedReq / FwdAux pair for a volume already on the device.
-void staged_request(int n, int pitch, int ndir, int nshift, int L, const float2 *pairs,
-                    const float *vol, const double *dir, const float *dir32,
+void staged_request(int n, int pitch, int ndir, int nshift, int L, int storage,
+                    const void *pairs, const void *vol, const double *dir, const float *dir32,
                     const double *shift, const float *shift32, double *out, StagedReq *r);
 
 // Ray kernels (k_ray.cu).
@@ -295,6 +303,9 @@ __device__ __forceinline__ double lin64(double t, double a, double b) {
 __device__ __forceinline__ float ldv(const float *v, int n, int ix, int iy, int iz) {
   return __ldg(v + ((size_t)ix * n + iy) * n + iz);
 }
+__device__ __forceinline__ float ldv(const __nv_bfloat16 *v, int n, int ix, int iy, int iz) {
+  return __bfloat162float(__ldg(v + ((size_t)ix * n + iy) * n + iz));
+}
 
 // fmod(x, y) for x >= 0, y > 0 and x / y < 2^52: the exact remainder x - n y,
 // n = trunc(x / y).  The quotient estimate from the rounded division is off
@@ -314,8 +325,9 @@ __device__ __forceinline__ double exact_rem(double x, double y) {
 }
 
 // cube_trilinear_interp, radon_grid/src/interp.c:25-60.
-static __device__ __noinline__ double exact_trilinear(const float *v, int n, double x, double y,
-                                               double z) {
+template <typename T>
+static __device__ __noinline__ double exact_trilinear(const T *v, int n, double x, double y,
+                                                      double z) {
   if ((fabs(x) > 1.0) || (fabs(y) > 1.0) || (fabs(z) > 1.0)) return 0.0;
   const double delta = __ddiv_rn(2.0, (double)(n - 1));
   const double x1 = __dadd_rn(x, 1.0), y1 = __dadd_rn(y, 1.0), z1 = __dadd_rn(z, 1.0);
