@@ -295,7 +295,9 @@ int wrt_server_create(const wrt_server_opts *opts, wrt_server **out);
 int wrt_server_submit(wrt_server *srv, const wrt_request *req, uint64_t *id);
 /* Waits up to timeout_ms (< 0: without limit, 0: poll) for a request; on
  * completion fills info (may be NULL), forgets the id and returns the
- * request's status; WRT_ERR_TIMEOUT if it is still running. */
+ * request's status; WRT_ERR_TIMEOUT if it is still running.  Each id is
+ * waited for once (a second wait returns WRT_ERR_NOT_FOUND); a request never
+ * waited for keeps its record until wrt_server_destroy. */
 int wrt_server_wait(wrt_server *srv, uint64_t id, int timeout_ms, wrt_request_info *info);
 int wrt_server_get_stats(wrt_server *srv, wrt_server_stats *stats);
 /* Finishes the launches in flight, cancels queued requests

@@ -207,11 +207,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                         unsigned long long *__restrict__ counter) {
   constexpr int kLanesPerRow = 32 / kGroup;
   constexpr int kWarps = kThreads / 32;
-  extern __shared__ float4 quads[];
-  __shared__ int s_item, s_dir;
-  __shared__ unsigned char s_rowlane[kWarps][32];  // compacted non-empty rows -> lane
+  // dynamic shared memory: per warp a row table and a guard-band queue, then
+  // the staged tile
+  extern __shared__ float4 dyn_smem[];
+  // the warp's compacted non-empty rows: (q0x, q0y, tz, jlo) and (jhi, shift
+  // index, i, whole row in the z band)
+  float4(*s_rows)[32][2] = reinterpret_cast<float4(*)[32][2]>(dyn_smem);
   // guard-band samples waiting for the FP64 path: (shift index, i << 16 | j)
-  __shared__ int2 s_xq[kWarps][64];
+  int2(*s_xq)[64] = reinterpret_cast<int2(*)[64]>(dyn_smem + kWarps * 64);
+  float4 *quads = dyn_smem + kWarps * wrt::kStagedWarpSmemQuads;
+  __shared__ int s_item, s_dir;
   // FP64 row geometry: per item (h, 1/h, layer bounds) and per warp's direction
   // (normal, delta v1, 1/(delta v1z))
   __shared__ double s_item_geo[4];
@@ -379,27 +384,40 @@ __global__ void __launch_bounds__(kThreads, 1)
               }
             }
           }
-          // ---- compact the non-empty rows (in row order) and walk them kGroup at a time
+          // ---- the non-empty rows, longest first (rows walked together then
+          // have similar lengths), kGroup at a time
           const bool live_row = valid && jlo <= jhi;
-          const unsigned rows = __ballot_sync(kFull, live_row);
-          const int nrows = __popc(rows);
-          if (live_row) s_rowlane[warp][__popc(rows & ((1u << lane) - 1u))] = (unsigned char)lane;
+          const int nrows = __popc(__ballot_sync(kFull, live_row));
+          if (live_row) {
+            float4 *rec = s_rows[warp][lane];
+            rec[0] = make_float4(ub, vb, tz, __int_as_float(jlo));
+            rec[1] = make_float4(__int_as_float(jhi), __int_as_float(is), __int_as_float(i),
+                                 __int_as_float((int)zexact));
+          }
+          // bitonic sort of (length, lane) keys, descending; empty rows last
+          unsigned key = live_row ? ((unsigned)(jhi - jlo + 1) << 5) | (unsigned)lane : 0u;
+#pragma unroll
+          for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+              const unsigned other = __shfl_xor_sync(kFull, key, j);
+              const bool up = ((lane & k) == 0) == ((lane & j) == 0);
+              key = up ? max(key, other) : min(key, other);
+            }
+          }
           __syncwarp();
           for (int g0 = 0; g0 < nrows; g0 += kGroup) {
             const int kr = g0 + lane / kLanesPerRow;
             const bool rvalid = kr < nrows;
-            const int src = rvalid ? s_rowlane[warp][kr] : 0;
-            const int k_is = __shfl_sync(kFull, is, src), k_i = __shfl_sync(kFull, i, src);
-            // (every lane takes part in every shuffle; the row's validity is
-            // applied afterwards)
-            const int k_jlo = __shfl_sync(kFull, jlo, src);
-            const int jhi_src = __shfl_sync(kFull, jhi, src);
-            const float k_ubm = __shfl_sync(kFull, ub, src);  // q - 1/2 at j = 0
-            const float k_vbm = __shfl_sync(kFull, vb, src);
-            const float k_tz = __shfl_sync(kFull, tz, src);
-            const int zx_src = __shfl_sync(kFull, (int)zexact, src);
-            const int k_jhi = rvalid ? jhi_src : k_jlo - 1;
-            const bool k_zx = rvalid && zx_src != 0;
+            const int slot = (int)(__shfl_sync(kFull, key, rvalid ? kr : 0) & 31u);
+            const float4 *rec = s_rows[warp][slot];
+            const float4 r0v = rec[0], r1v = rec[1];
+            const float k_ubm = r0v.x, k_vbm = r0v.y;  // q - 1/2 at j = 0
+            const float k_tz = r0v.z;
+            const int k_jlo = __float_as_int(r0v.w);
+            const int k_jhi = rvalid ? __float_as_int(r1v.x) : k_jlo - 1;
+            const int k_is = __float_as_int(r1v.y), k_i = __float_as_int(r1v.z);
+            const bool k_zx = rvalid && __float_as_int(r1v.w) != 0;
             const u64 qb = pk2(k_ubm, k_vbm), tz2 = pk2(k_tz, k_tz);
             const int len = k_jhi - k_jlo + 1;
             const int trips = (int)__reduce_max_sync(
@@ -534,6 +552,7 @@ int launch_cfg(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
                const StagedItem *d_items, const int *d_nitems, int max_smem, int *d_next) {
   const bool count = ctx->d_counter != nullptr;
   auto kern = count ? plane_staged_kernel<T, G, K, true> : plane_staged_kernel<T, G, K, false>;
+  max_smem += (T / 32) * wrt::kStagedWarpSmemQuads * 16;  // per-warp row tables and queues
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged kernel smem attribute");
   e = cudaMemsetAsync(d_next, 0, sizeof(int), stream);

@@ -142,7 +142,11 @@ inline float staged_guard(int n, int L) {
   return 3.0e-7f * (float)(n > 32 ? n : 32) + 6.0e-8f * (float)L;
 }
 constexpr int kStagedDirChunk = 512;  // directions per work item
-constexpr int kStagedSmemMax = 200 * 1024;  // staged tile budget (bytes of shared memory)
+// Staged tile budget (bytes of dynamic shared memory): 227 KB per CTA minus
+// the per-warp row tables and guard-band queues (kStagedWarpSmemQuads float4
+// per warp, 48 KB at 1024 threads) and a few static words.
+constexpr int kStagedSmemMax = 168 * 1024;
+constexpr int kStagedWarpSmemQuads = 96;
 int plane_staged_launch(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
                         const StagedItem *d_items, const int *d_nitems, int max_smem,
                         int *d_next);
