@@ -243,7 +243,7 @@ def run_reference(args, dist):
 # ------------------------------------------------------------ our arm
 def traffic_from_profiles():
     """DRAM bytes per launch of the plane kernel from the committed ncu summary."""
-    f = ROOT / "profiles" / "plane_kernel_128cubed.md"
+    f = ROOT / "profiles" / "plane_staged_kernel_128cubed.md"
     if not f.exists():
         return None
     for ln in f.read_text().splitlines():

@@ -869,22 +869,22 @@ int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
   std::vector<double> phi(nphi), theta(ntheta), w(ntheta), shift(nshift);
   st = sphere_grid(ctx, nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), shift.data());
   const int ndir = nphi * ntheta;
-  std::vector<float4> dirw(ndir);
+  std::vector<double4> dirw(ndir);
   const double dphi = 2 * M_PI / nphi;  // backprojection/C/src/integral.c:11
   for (int ip = 0; ip < nphi; ++ip)
     for (int it = 0; it < ntheta; ++it)
-      dirw[ip * ntheta + it] = make_float4((float)(sin(theta[it]) * cos(phi[ip])),
-                                           (float)(sin(theta[it]) * sin(phi[ip])),
-                                           (float)cos(theta[it]), (float)(dphi * w[it]));
+      dirw[ip * ntheta + it] = make_double4(sin(theta[it]) * cos(phi[ip]),
+                                            sin(theta[it]) * sin(phi[ip]), cos(theta[it]),
+                                            dphi * w[it]);
   DevBuf dradon(ctx), ddirw(ctx), dout(ctx);
   const size_t nin = (size_t)nshift * ndir, nout = (size_t)ngrid * ngrid * ngrid;
   if (!st) st = dradon.alloc(sizeof(double) * nin);
-  if (!st) st = ddirw.alloc(sizeof(float4) * ndir);
+  if (!st) st = ddirw.alloc(sizeof(double4) * ndir);
   if (!st) st = dout.alloc(sizeof(double) * nout);
   if (!st) st = h2d(ctx, dradon.p, radon, sizeof(double) * nin, "adjoint input");
-  if (!st) st = h2d(ctx, ddirw.p, dirw.data(), sizeof(float4) * ndir, "adjoint directions");
+  if (!st) st = h2d(ctx, ddirw.p, dirw.data(), sizeof(double4) * ndir, "adjoint directions");
   if (!st)
-    st = adjoint_forward(ctx, dradon.as<double>(), nphi, ntheta, nshift, ddirw.as<float4>(), ngrid,
+    st = adjoint_forward(ctx, dradon.as<double>(), nphi, ntheta, nshift, ddirw.as<double4>(), ngrid,
                          dout.as<double>());
   if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "adjoint result");
   return st;

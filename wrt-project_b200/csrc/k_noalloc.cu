@@ -30,7 +30,7 @@ int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, i
                          const double *d_cp, const double *d_den, double *d_scratch,
                          float4 *d_lines);
 int launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int ntheta, int nshift,
-                   const float4 *d_dirw, int n, double *d_out);
+                   const double4 *d_dirw, int n, double *d_out);
 }  // namespace wrt
 
 namespace {
@@ -44,11 +44,11 @@ constexpr size_t kOffW = align256(kOffX + sizeof(double) * kMaxTheta);
 constexpr size_t kOffCp = align256(kOffW + sizeof(double) * kMaxTheta);
 constexpr size_t kOffDen = align256(kOffCp + sizeof(double) * kMaxShift);
 constexpr size_t kOffDirw = align256(kOffDen + sizeof(double) * kMaxShift);
-constexpr size_t kOffM = align256(kOffDirw + sizeof(float4) * kMaxDirs);
+constexpr size_t kOffM = align256(kOffDirw + sizeof(double4) * kMaxDirs);
 constexpr size_t kOffLines = align256(kOffM + sizeof(double) * kMaxEntries);
 constexpr size_t kScratchBytes = align256(kOffLines + sizeof(float4) * kMaxEntries);
 
-// The working memory (about 6.3 MB).  In host code this name is a host-side
+// The working memory (about 6.6 MB).  In host code this name is a host-side
 // stand-in, not a device address: host code must use the address returned by
 // cudaGetSymbolAddress (scratch_base below).
 static __device__ __align__(256) unsigned char g_adjoint_scratch[kScratchBytes];
@@ -72,14 +72,13 @@ __global__ void spline_coef_kernel(int ns, double *cp, double *den) {
 // t = acos(GL node), p = 2 pi ip / nphi
 // (backprojection/C/src/init.c:222-245 and integral.c:11-18).
 __global__ void direction_weights_kernel(int nphi, int ntheta, const double *x, const double *w,
-                                         float4 *dirw) {
+                                         double4 *dirw) {
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= nphi * ntheta) return;
   const int ip = d / ntheta, it = d - ip * ntheta;
   const double dphi = (2 * WRT_PI) / nphi;
   const double p = dphi * ip, t = acos(x[it]);
-  dirw[d] = make_float4((float)(sin(t) * cos(p)), (float)(sin(t) * sin(p)), (float)cos(t),
-                        (float)(dphi * w[it]));
+  dirw[d] = make_double4(sin(t) * cos(p), sin(t) * sin(p), cos(t), dphi * w[it]);
 }
 
 std::mutex g_setup_mutex;
@@ -124,7 +123,7 @@ extern "C" int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, i
   double *w = reinterpret_cast<double *>(base + kOffW);
   double *cp = reinterpret_cast<double *>(base + kOffCp);
   double *den = reinterpret_cast<double *>(base + kOffDen);
-  float4 *dirw = reinterpret_cast<float4 *>(base + kOffDirw);
+  double4 *dirw = reinterpret_cast<double4 *>(base + kOffDirw);
   double *M = reinterpret_cast<double *>(base + kOffM);
   float4 *lines = reinterpret_cast<float4 *>(base + kOffLines);
   cudaStream_t s = ctx->stream;

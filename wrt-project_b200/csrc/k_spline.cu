@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256)
 // directions.  dirw[d] = (sin t cos p, sin t sin p, cos t, dphi * w_t).
 __global__ void __launch_bounds__(256)
     adjoint_kernel(const float4 *__restrict__ lines /* [d][ns-1] */, int ndir, int ntheta, int ns,
-                   const float4 *__restrict__ dirw, int n, double *__restrict__ out) {
+                   const double4 *__restrict__ dirw, int n, double *__restrict__ out) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long total = (long long)n * n * n;
   if (k >= total) return;
@@ -164,7 +164,7 @@ int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, i
 }
 
 int launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int ntheta, int nshift,
-                   const float4 *d_dirw, int n, double *d_out) {
+                   const double4 *d_dirw, int n, double *d_out) {
   const long long total = (long long)n * n * n;
   adjoint_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_lines, ndir, ntheta,
                                                                         nshift, d_dirw, n, d_out);
@@ -195,7 +195,7 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
 }
 
 int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
-                    const float4 *d_dirw, int n, double *d_out) {
+                    const double4 *d_dirw, int n, double *d_out) {
   // lines (iphi, itheta): element is at d_radon[(is*nphi + iphi)*ntheta + itheta]
   float4 *d_lines = nullptr;
   size_t bytes = 0;

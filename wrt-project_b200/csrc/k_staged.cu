@@ -31,12 +31,11 @@
 // the reference's FP64 arithmetic from global memory (in a second pass over
 // the rows that have such samples, outside the hot loop).  Every row belongs
 // to exactly one layer and every sample to exactly one tile, decided by the
-// same FP32 expressions everywhere.  A lane sums its samples of one plane in
-// FP32, the warp combines the lanes in a fixed tree, and the plane's sums
-// over items are accumulated as 64-bit fixed-point integers (scale 2^k from
-// max|f| so that no sum can overflow): the result does not depend on the
-// order in which items and atomics complete -- bitwise identical alone or in
-// a batch.
+// same FP32 expressions everywhere.  The lanes of a row sum its samples in
+// FP32 and combine in a fixed tree; the row total is added to its plane as a
+// 64-bit fixed-point integer (scale 2^k from max|f| so that no sum can
+// overflow): the result does not depend on the order in which rows, items and
+// atomics complete -- bitwise identical alone or in a batch.
 #include <math.h>
 #include <string.h>
 
@@ -427,7 +426,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool any_band = k_zx;
             float part = 0.0f;
             {
+              // a row in the z band has no fast samples: its last fast j is jlo - 1
+              const float jhif_fast = k_zx ? jf0 - 1.0f : jhif;
               u64 jj = pk2(jf0, jf0);
+#pragma unroll 2
               for (int t = 0; t < trips; ++t, jj = add2(jj, step2)) {
                 float jf, jf_hi;
                 upk2(jj, jf, jf_hi);
@@ -435,9 +437,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 float sx, sy;
                 upk2(c.s, sx, sy);
                 const int iyr = __float_as_int(sy) - yoff;
-                const bool live = jf <= jhif;
+                const bool live = jf <= jhif_fast;
                 any_band |= live & c.band;
-                if (live & !(c.band | k_zx) & ((unsigned)iyr < (unsigned)H)) {
+                if (live & !c.band & ((unsigned)iyr < (unsigned)H)) {
                   const unsigned a = sbase + 16u * (unsigned)(iyr * qp + __float_as_int(sx));
                   u64 a01, a23, b01, b23;
                   lds_pairs(a, a01, a23);
@@ -484,22 +486,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
               }
             }
-            // ---- row sums over the row's lanes, fixed point, then the rows
-            // of one plane combined (rows are in plane order) and one atomic
-            // per plane segment
+            // ---- row sums over the row's lanes, fixed point, one atomic per row
 #pragma unroll
             for (int o = kLanesPerRow / 2; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
-            long long v = rvalid ? __double2ll_rn((double)part * R.scale) : 0LL;
-            const int key = rvalid ? k_is : -1;
-#pragma unroll
-            for (int o = kLanesPerRow; o < 32; o <<= 1) {
-              const long long tv = __shfl_up_sync(kFull, v, o);
-              const int k2 = __shfl_up_sync(kFull, key, o);
-              if (lane >= o && k2 == key) v += tv;
-            }
-            const int knext = kLanesPerRow < 32 ? __shfl_down_sync(kFull, key, kLanesPerRow) : -2;
-            const bool last = lane >= 32 - kLanesPerRow || knext != key;
-            if (rvalid && pos == 0 && last && v != 0)
+            const long long v = rvalid ? __double2ll_rn((double)part * R.scale) : 0LL;
+            if (pos == 0 && v != 0)
               atomicAdd(R.acc + (size_t)k_is * R.ndir + d, (unsigned long long)v);
           }
           __syncwarp();

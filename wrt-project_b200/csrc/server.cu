@@ -53,7 +53,7 @@ struct GridTables {
   float *dir32 = nullptr;    // [ndir][8]
   double *shift = nullptr;   // [nshift]
   float *shift32 = nullptr;  // [nshift]
-  float4 *dirw = nullptr;    // [ndir]
+  double4 *dirw = nullptr;   // [ndir]
   double *cp = nullptr, *den = nullptr;  // [nshift]
   int nphi = 0, ntheta = 0, nshift = 0;
   int refs = 0;
@@ -129,7 +129,7 @@ size_t request_bytes(const wrt_request &r) {
 size_t grid_bytes(int nphi, int ntheta, int nshift) {
   const size_t ndir = (size_t)nphi * ntheta;
   return al(72 * ndir) + al(32 * ndir) + al(8 * (size_t)nshift) + al(4 * (size_t)nshift) +
-         al(16 * ndir) + 2 * al(8 * (size_t)nshift);
+         al(32 * ndir) + 2 * al(8 * (size_t)nshift);
 }
 
 // ---------------------------------------------------------------- grids
@@ -149,13 +149,13 @@ int make_grid(wrt_server *s, GridTables &g) {
   for (int i = 0; i < nshift; ++i) shift32[i] = (float)shift[i];
   // backprojection weights (backprojection/C/src/integral.c:11-18) and the
   // natural-spline elimination coefficients
-  std::vector<float4> dirw(ndir);
+  std::vector<double4> dirw(ndir);
   const double dphi = 2 * M_PI / nphi;
   for (int ip = 0; ip < nphi; ++ip)
     for (int it = 0; it < ntheta; ++it)
-      dirw[ip * ntheta + it] = make_float4((float)(sin(theta[it]) * cos(phi[ip])),
-                                           (float)(sin(theta[it]) * sin(phi[ip])),
-                                           (float)cos(theta[it]), (float)(dphi * w[it]));
+      dirw[ip * ntheta + it] = make_double4(sin(theta[it]) * cos(phi[ip]),
+                                            sin(theta[it]) * sin(phi[ip]), cos(theta[it]),
+                                            dphi * w[it]);
   std::vector<double> cp(nshift, 0.0), den(nshift, 1.0);
   for (int i = 1; i + 1 < nshift; ++i) {
     den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);
@@ -172,7 +172,7 @@ int make_grid(wrt_server *s, GridTables &g) {
   g.dir32 = reinterpret_cast<float *>(place(32 * ndir));
   g.shift = reinterpret_cast<double *>(place(8 * (size_t)nshift));
   g.shift32 = reinterpret_cast<float *>(place(4 * (size_t)nshift));
-  g.dirw = reinterpret_cast<float4 *>(place(16 * ndir));
+  g.dirw = reinterpret_cast<double4 *>(place(32 * ndir));
   g.cp = reinterpret_cast<double *>(place(8 * (size_t)nshift));
   g.den = reinterpret_cast<double *>(place(8 * (size_t)nshift));
   struct {
@@ -181,7 +181,7 @@ int make_grid(wrt_server *s, GridTables &g) {
     size_t bytes;
   } copies[] = {{g.dir, dir.data(), 72 * ndir},          {g.dir32, dir32.data(), 32 * ndir},
                 {g.shift, shift.data(), 8 * (size_t)nshift}, {g.shift32, shift32.data(), 4 * (size_t)nshift},
-                {g.dirw, dirw.data(), 16 * ndir},         {g.cp, cp.data(), 8 * (size_t)nshift},
+                {g.dirw, dirw.data(), 32 * ndir},         {g.cp, cp.data(), 8 * (size_t)nshift},
                 {g.den, den.data(), 8 * (size_t)nshift}};
   for (auto &c : copies) {
     cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, ctx->stream);

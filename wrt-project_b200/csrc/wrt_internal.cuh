@@ -178,7 +178,7 @@ struct FwdAux {                    // per forward request, beside its StagedReq
 };
 struct AdjReq {                    // one backprojection
   const double *radon;             // [is][iphi][itheta]
-  const float4 *dirw;              // [ndir]: omega, dphi * w_theta
+  const double4 *dirw;             // [ndir]: omega, dphi * w_theta (FP64)
   const double *cp, *den;          // spline elimination coefficients [nshift]
   double *scratch;                 // [ndir][nshift]
   float4 *lines;                   // [ndir][nshift - 1]
@@ -260,7 +260,7 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
                       const double *d_cs /* [ntheta][2]: cos, sin theta */, int ntheta,
                       double *d_out);
 int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
-                    const float4 *d_dirw /* [nphi*ntheta]: omega, dphi*w */, int n,
+                    const double4 *d_dirw /* [nphi*ntheta]: omega, dphi*w */, int n,
                     double *d_out);
 
 }  // namespace wrt
