@@ -546,8 +546,8 @@ int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, in
   r.ndir = grid->nphi * grid->ntheta;
   r.nshift = grid->nshift;
   r.L = L;
-  r.guard = staged_guard(n, L);
   r.crop_r2 = trilinear_crop_r2(vol->r2, n);
+  r.guard = staged_guard(n, L, r.crop_r2);
   r.scale = fixed_point_scale(vol->maxabs, L);
   StagedItem *d_items = nullptr;
   const int *d_nitems = nullptr;

@@ -121,6 +121,7 @@ __global__ void batch_request_kernel(char *t) {
   const float maxabs = __uint_as_float(A[r].stats[1]);
   const int n = A[r].n;
   F[r].crop_r2 = wrt::trilinear_crop_r2(r2, n);
+  F[r].guard = wrt::staged_guard(n, A[r].L, F[r].crop_r2);
   F[r].scale = wrt::fixed_point_scale(maxabs, A[r].L);
   const double delta = 1.0 / n;
   A[r].factor = delta * delta / F[r].scale;
@@ -197,8 +198,8 @@ void staged_request(int n, int pitch, int ndir, int nshift, int L, int storage,
   r->nshift = nshift;
   r->L = L;
   r->storage = storage;
-  r->guard = staged_guard(n, L);
-  r->crop_r2 = 3.0f + 1e-5f;
+  r->crop_r2 = 3.0f + 1e-5f;  // set from the volume statistics by the launch
+  r->guard = staged_guard(n, L, r->crop_r2);
   r->scale = 1.0;
 }
 

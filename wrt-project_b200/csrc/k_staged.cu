@@ -278,10 +278,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     const float halfband = 0.5f - g;
     const float rc2 = R.crop_r2;
     const int L = R.L;
-    // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x + magic))
-    const unsigned sbase = smem0 + 16u * (unsigned)(kPadX - kMagicBits);
+    // Cell coordinates are held relative to the grid's centre cell C (halves
+    // their magnitude and so their FP32 rounding, which sets the guard band).
+    const int C = W / 2;
+    // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x' + magic))
+    const unsigned sbase = smem0 + 16u * (unsigned)(kPadX + C - kMagicBits);
     const unsigned qp16 = 16u * (unsigned)qp;
-    const int yoff = kMagicBits + y0;
+    const int yoff = kMagicBits - C + y0;
     for (;;) {
       int dl = 0;
       if (lane == 0) dl = atomicAdd(&s_dir, 1);
@@ -368,16 +371,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             const double tz64 = row_w(s64, ldsd(G + 2), ldsd(G + 5), di64, h64) - (double)item.layer;
             tz = (float)tz64;
             zexact = tz64 < kZBand || tz64 > 1.0 - kZBand;
-            // row origin in cell units (q - 1/2 at j = 0), FP64 then rounded once
-            ub = (float)((fma(di64, ldsd(G + 3), s64 * ldsd(G + 0)) + 1.0) * h64 - 0.5);
-            vb = (float)((fma(di64, ldsd(G + 4), s64 * ldsd(G + 1)) + 1.0) * h64 - 0.5);
+            // row origin in cell units relative to the centre (q - 1/2 - C at
+            // j = 0), FP64 then rounded once
+            ub = (float)((fma(di64, ldsd(G + 3), s64 * ldsd(G + 0)) + 1.0) * h64 - (0.5 + C));
+            vb = (float)((fma(di64, ldsd(G + 4), s64 * ldsd(G + 1)) + 1.0) * h64 - (0.5 + C));
             const float rem = rc2 - s * s - (delta * di) * (delta * di);
             if (rem >= 0.0f) {
               const int jm = (int)floorf(sqrtf(rem) / delta) + 1;
               jlo = max(-L, -jm);
               jhi = min(L - 1, jm);
-              if (!clip_lin(ub, du, inv_du, -1.5f, (float)n - 0.5f, jlo, jhi) ||
-                  !clip_lin(vb, dv, inv_dv, (float)y0 - 1.5f, (float)(y0 + H) + 0.5f, jlo, jhi)) {
+              if (!clip_lin(ub, du, inv_du, -1.5f - C, (float)(n - C) - 0.5f, jlo, jhi) ||
+                  !clip_lin(vb, dv, inv_dv, (float)(y0 - C) - 1.5f, (float)(y0 + H - C) + 0.5f,
+                            jlo, jhi)) {
                 jlo = 1;
                 jhi = 0;
               }
@@ -467,7 +472,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 // a guard-band sample belongs to the tile of its FP32 cell row,
                 // clamped to the grid (samples within the band outside a face
                 // are evaluated, and cut off, by the FP64 reference arithmetic)
-                const int cy = min(max(__float_as_int(sy) - kMagicBits, 0), W - 1) - y0;
+                const int cy = min(max(__float_as_int(sy) - kMagicBits + C, 0), W - 1) - y0;
                 const bool want = (jf <= jhif) & (c.band | k_zx) & ((unsigned)cy < (unsigned)H);
                 const unsigned m = __ballot_sync(kFull, want);
                 if (m) {
@@ -557,8 +562,10 @@ int launch_cfg(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
 
 // The tile shapes the autotuner chooses among: (CTA threads, lattice rows a
 // warp walks at once, shifts per lane per enumeration pass).
+// Entry 0 is the default (no tuning: the serving loop, untuned contexts); it
+// was the fastest at 96^3, 128^3 and 256^3 on B200.
 const StagedConfig kStagedConfigs[] = {
-    {768, 8, 2}, {768, 4, 2}, {1024, 8, 2}, {1024, 4, 2}, {768, 2, 2}, {1024, 1, 2}, {512, 8, 4},
+    {1024, 8, 2}, {768, 8, 2}, {768, 4, 2}, {1024, 4, 2}, {768, 2, 2}, {1024, 1, 2}, {512, 8, 4},
 };
 const int kNumStagedConfigs = sizeof(kStagedConfigs) / sizeof(kStagedConfigs[0]);
 
@@ -568,9 +575,9 @@ int plane_staged_launch(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_re
   const int c = (ctx->staged_config >= 0 && ctx->staged_config < kNumStagedConfigs)
                     ? ctx->staged_config : 0;
   switch (c) {
-    case 0: return launch_cfg<768, 8, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
-    case 1: return launch_cfg<768, 4, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
-    case 2: return launch_cfg<1024, 8, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 0: return launch_cfg<1024, 8, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 1: return launch_cfg<768, 8, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+    case 2: return launch_cfg<768, 4, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
     case 3: return launch_cfg<1024, 4, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
     case 4: return launch_cfg<768, 2, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
     case 5: return launch_cfg<1024, 1, 2>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);

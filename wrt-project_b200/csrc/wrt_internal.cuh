@@ -131,15 +131,22 @@ struct StagedConfig {
 extern const StagedConfig kStagedConfigs[];
 extern const int kNumStagedConfigs;
 int staged_smem_bytes(int n, int *tile_h, int *qpitch);
-// Guard band (in cells) of the staged kernel's x / y cell fractions.  Its
-// FP32 cell coordinate q = fma(j, du, q0) has q0 and du rounded once from
-// FP64, so |q - q_exact| <= 0.5 ulp(q0) + |j| |du| 2^-24 + 0.5 ulp(q) with
-// |q0| < 1.4 n, |du| < 1/2, |j| <= L: below 1.4e-7 n + 3e-8 L.  The band is
-// twice that, so every sample whose exact coordinate is on a cell boundary
-// (where the reference's cell index and fraction can disagree) or on a cube
-// face lies inside it.
-inline float staged_guard(int n, int L) {
-  return 3.0e-7f * (float)(n > 32 ? n : 32) + 6.0e-8f * (float)L;
+// Guard band (in cells) of the staged kernel's x / y cell fractions.  Cell
+// coordinates are held relative to the centre cell C = (n-1)/2 (rounded
+// down); q' = fma(j, du, q0') with q0' and du rounded once from FP64, so
+// |q' - q'_exact| <= 0.5 ulp(q0') + |j| |du| 2^-24 + 0.5 ulp(q') where
+// |q0'| <= sqrt(crop_r2) h + 1 (the row's j = 0 point lies in the crop
+// ball), |q'| <= h + 3 for every sample evaluated, |du| < 1/2 and |j| <= L.
+// The band is twice that bound, so every sample whose exact coordinate is on
+// a cell boundary (where the reference's cell index and fraction can
+// disagree) or on a cube face lies inside it.  Host and device compute it
+// alike (the batched path sets it on the device from the volume statistics).
+__host__ __device__ inline float staged_guard(int n, int L, float crop_r2) {
+  const double h = 0.5 * (n - 1);
+  const double ulp = 1.0 / 8388608.0;  // 2^-23 relative
+  const double bound = 0.5 * ulp * (sqrt((double)crop_r2) * h + 1.0) +
+                       0.5 * ulp * (h + 3.0) + 0.5 * ulp * 0.5 * L;
+  return (float)(2.0 * bound) + 1e-7f;
 }
 constexpr int kStagedDirChunk = 512;  // directions per work item
 // Staged tile budget (bytes of dynamic shared memory): 227 KB per CTA minus
