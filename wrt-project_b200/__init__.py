@@ -18,7 +18,9 @@ missing library or device raises ``WrtError``.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -84,6 +86,10 @@ _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _vp, _i, _sz = C.c_void_p, C.c_int, C.c_size_t
 
 _lib = None
+# contexts and servers still open; closed in order at interpreter exit, while
+# this module is intact (objects left to the garbage collector at shutdown
+# would otherwise be finalised in no particular order)
+_live = weakref.WeakSet()
 
 
 def lib() -> C.CDLL:
@@ -166,17 +172,26 @@ class Context:
 
     def __init__(self, device: int = 0, budget_bytes: int = 0):
         self._h = _vp()
+        self._children = weakref.WeakSet()  # resources created in this context
         st = lib().wrt_ctx_create(int(device), int(budget_bytes), C.byref(self._h))
         if st:
             raise WrtError(st, "wrt_ctx_create")
+        _live.add(self)
 
     # -- plumbing
     @property
     def handle(self):
         return self._h
 
+    def _adopt(self, obj):
+        self._children.add(obj)
+
     def close(self):
+        """Destroy the context; resources still open in it are closed first
+        (the C library requires that order)."""
         if self._h:
+            for c in list(self._children):
+                c.close()
             lib().wrt_ctx_destroy(self._h)
             self._h = _vp()
 
@@ -297,6 +312,7 @@ class DeviceBuffer:
     def __init__(self, ctx: Context, nbytes: int):
         self.ctx, self.nbytes, self._p = ctx, int(nbytes), _vp()
         ctx.check(lib().wrt_device_alloc(ctx.handle, self.nbytes, C.byref(self._p)), "device_alloc")
+        ctx._adopt(self)
 
     @property
     def ptr(self) -> int:
@@ -316,7 +332,8 @@ class DeviceBuffer:
 
     def close(self):
         if self._p:
-            lib().wrt_device_free(self.ctx.handle, self._p)
+            if self.ctx.handle:
+                lib().wrt_device_free(self.ctx.handle, self._p)
             self._p = _vp()
 
     def __del__(self):
@@ -334,13 +351,15 @@ class PinnedArray:
         dt = np.dtype(dtype)
         nbytes = int(np.prod(shape)) * dt.itemsize
         ctx.check(lib().wrt_host_alloc_pinned(ctx.handle, nbytes, C.byref(self._p)), "pinned")
+        ctx._adopt(self)
         buf = (C.c_char * nbytes).from_address(self._p.value)
         self.array = np.frombuffer(buf, dtype=dt).reshape(shape)
 
     def close(self):
         if self._p:
             self.array = None
-            lib().wrt_host_free_pinned(self.ctx.handle, self._p)
+            if self.ctx.handle:
+                lib().wrt_host_free_pinned(self.ctx.handle, self._p)
             self._p = _vp()
 
     def __del__(self):
@@ -359,6 +378,7 @@ class Volume:
         self.storage = int(storage)
         ctx.check(lib().wrt_volume_create_storage(ctx.handle, self.n, self.storage,
                                                   C.byref(self._h)), "volume_create")
+        ctx._adopt(self)
 
     @property
     def nbytes(self) -> int:
@@ -381,7 +401,8 @@ class Volume:
 
     def close(self):
         if self._h:
-            lib().wrt_volume_destroy(self._h)
+            if self.ctx.handle:
+                lib().wrt_volume_destroy(self._h)
             self._h = _vp()
 
     def __del__(self):
@@ -399,6 +420,7 @@ class Grid:
         self.nphi, self.ntheta, self.nshift = int(nphi), int(ntheta), int(nshift)
         ctx.check(lib().wrt_grid_create(ctx.handle, self.nphi, self.ntheta, self.nshift,
                                         C.byref(self._h)), "grid_create")
+        ctx._adopt(self)
 
     @property
     def handle(self):
@@ -410,7 +432,8 @@ class Grid:
 
     def close(self):
         if self._h:
-            lib().wrt_grid_destroy(self._h)
+            if self.ctx.handle:
+                lib().wrt_grid_destroy(self._h)
             self._h = _vp()
 
     def __del__(self):
@@ -481,6 +504,7 @@ class Server:
         if st:
             raise WrtError(st, "wrt_server_create")
         self._keep = {}
+        _live.add(self)
 
     def submit_forward(self, volume, nphi, ntheta, nshift, out, half_extent=0, tag=0) -> int:
         """volume: float32 [n][n][n]; out: float64 [nshift][nphi][ntheta]."""
@@ -540,6 +564,20 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def _close_all():
+    """Servers first (their threads use their own contexts), then contexts
+    (each closes its resources before itself)."""
+    objs = sorted(list(_live), key=lambda o: not isinstance(o, Server))
+    for o in objs:
+        try:
+            o.close()
+        except Exception:
+            pass
+
+
+atexit.register(_close_all)
 
 
 def round_bf16(a) -> np.ndarray:
