@@ -15,9 +15,11 @@
 //   zeros pad every staged row on both sides in x, so samples just outside
 //   the cube's x faces read zeros and need no bounds test.  The warps take the
 //   chunk's directions one at a time, enumerate every lattice row (shift s,
-//   index i) of that direction whose z falls in layer iz, and walk each row
-//   with all 32 lanes on consecutive samples (neighbouring lanes read the
-//   same or adjacent cells: broadcasts, few bank conflicts).
+//   index i) of that direction whose z falls in layer iz, and walk them kGroup
+//   rows at a time, 32/kGroup lanes of a row on consecutive samples (those
+//   lanes read the same or adjacent cells, so bank conflicts come only from
+//   different rows in one quarter-warp; a warp's 16-byte shared load costs
+//   four wavefronts however much its lanes overlap).
 //   Persistent CTAs (one per SM) pull items from a global counter; the host
 //   orders items by estimated cost, largest first.
 //
@@ -147,6 +149,35 @@ __device__ __forceinline__ bool clip_lin(float q0, float dq, float inv, float lo
   return jlo <= jhi;
 }
 
+// Cell row of sample j of a row, relative to the tile (the fast loop's
+// expression bit for bit: q_y = fma(j, dv, vb) rounded once, then rounded to
+// an integer by the magic constant).  Monotone in j: non-decreasing for
+// dv >= 0, non-increasing for dv < 0.
+__device__ __forceinline__ int row_cell_y(int j, float vb, float dv, int yoff) {
+  return __float_as_int(__fadd_rn(__fmaf_rn((float)j, dv, vb), kMagic)) - yoff;
+}
+
+// First j in [lo, hi] with sgn * (row_cell_y(j) - c) >= 0 (hi + 1 if none);
+// the predicate is false then true as j grows.  jest: real-valued estimate of
+// the switch, corrected by at most three steps each way and verified against
+// its neighbours; a bisection settles the cases it does not (directions with
+// dv ~ 0, where the estimate means nothing).
+__device__ __forceinline__ int first_at_or_past(int lo, int hi, float jest, int c, int sgn,
+                                             float vb, float dv, int yoff) {
+  auto at = [&](int j) { return sgn * (row_cell_y(j, vb, dv, yoff) - c) >= 0; };
+  int j = (int)fminf(fmaxf(ceilf(jest), (float)lo), (float)hi + 1.0f);  // NaN -> lo
+  for (int k = 0; k < 3 && j > lo && at(j - 1); ++k) --j;
+  for (int k = 0; k < 3 && j <= hi && !at(j); ++k) ++j;
+  if ((j == lo || !at(j - 1)) && (j > hi || at(j))) return j;
+  int a = lo, b = hi + 1;
+  for (int k = 0; k < 32 && a < b; ++k) {
+    const int m = (a + b) >> 1;
+    if (at(m)) b = m;
+    else a = m + 1;
+  }
+  return a;
+}
+
 __device__ __noinline__ double exact_sample(const wrt::StagedReq &R, int d, int is, int i, int j) {
   const double *D = R.dir + 9 * (size_t)d;
   const double s = R.shift[is];
@@ -273,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     }
     __syncthreads();
-    const float delta = 1.0f / (float)n;
+    const float delta = 1.0f / (float)n, nf = (float)n;
     const float g = R.guard;
     const float halfband = 0.5f - g;
     const float rc2 = R.crop_r2;
@@ -281,10 +312,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     // Cell coordinates are held relative to the grid's centre cell C (halves
     // their magnitude and so their FP32 rounding, which sets the guard band).
     const int C = W / 2;
-    // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x' + magic))
+    // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x' + magic)),
+    // yrel = bits(y' + magic) - yoff; as one expression (mod 2^32):
+    //   bits(y' + magic) * 16 qp + 16 bits(x' + magic) + abase
     const unsigned sbase = smem0 + 16u * (unsigned)(kPadX + C - kMagicBits);
     const unsigned qp16 = 16u * (unsigned)qp;
     const int yoff = kMagicBits - C + y0;
+    const unsigned abase = sbase - qp16 * (unsigned)yoff;
     for (;;) {
       int dl = 0;
       if (lane == 0) dl = atomicAdd(&s_dir, 1);
@@ -319,7 +353,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const float s = __ldg(R.shift32 + is);
             const float rem = rc2 - s * s;
             if (rem >= 0.0f) {
-              const int im = (int)floorf(sqrtf(rem) / delta) + 1;
+              // |i| <= sqrt(rem) / delta; +1 covers the rounding of sqrt and n
+              const int im = (int)floorf(sqrtf(rem) * nf) + 1;
               cnt[k] = rows_in_layer(__ldg(R.shift + is), ldsd(G + 2), ldsd(G + 5), ldsd(G + 6),
                                      ldsd(&s_item_geo[0]), ldsd(&s_item_geo[1]),
                                      ldsd(&s_item_geo[2]), ldsd(&s_item_geo[3]), max(-L, -im),
@@ -359,10 +394,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (is < 0) off -= c;
           }
           const bool valid = r < total && is >= 0;
-          // ---- row set-up (one lane per row)
-          int jlo = 1, jhi = 0;
+          // ---- row set-up (one lane per row): [jlo, jhi] holds every sample
+          // of the row that this tile may have to evaluate; [ja, jb] is the
+          // exact run of samples whose FP32 cell row lies in the tile (the fast
+          // loop walks it without a per-sample tile test)
+          int jlo = 1, jhi = 0, ja = 1, jb = 0;
           float ub = 0.f, vb = 0.f, tz = 0.f;
-          bool zexact = false;
+          bool zexact = false, edge = false;
           if (valid) {
             const float s = __ldg(R.shift32 + is);
             const double s64 = __ldg(R.shift + is), di64 = (double)i;
@@ -377,7 +415,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             vb = (float)((fma(di64, ldsd(G + 4), s64 * ldsd(G + 1)) + 1.0) * h64 - (0.5 + C));
             const float rem = rc2 - s * s - (delta * di) * (delta * di);
             if (rem >= 0.0f) {
-              const int jm = (int)floorf(sqrtf(rem) / delta) + 1;
+              const int jm = (int)floorf(sqrtf(rem) * nf) + 1;
               jlo = max(-L, -jm);
               jhi = min(L - 1, jm);
               if (!clip_lin(ub, du, inv_du, -1.5f - C, (float)(n - C) - 0.5f, jlo, jhi) ||
@@ -387,19 +425,59 @@ __global__ void __launch_bounds__(kThreads, 1)
                 jhi = 0;
               }
             }
+            if (jlo <= jhi && zexact) {
+              ja = jlo;  // a row in the z band has no fast samples
+              jb = jlo - 1;
+            } else if (jlo <= jhi) {
+              const float yb = (float)(y0 - C) - 0.5f;  // q_y at the tile's first cell row
+              if (dv >= 0.0f) {
+                ja = first_at_or_past(jlo, jhi, (yb - vb) * inv_dv, 0, 1, vb, dv, yoff);
+                jb = first_at_or_past(jlo, jhi, (yb + (float)H - vb) * inv_dv, H, 1, vb, dv,
+                                      yoff) - 1;
+              } else {
+                ja = first_at_or_past(jlo, jhi, (yb + (float)H - vb) * inv_dv, H - 1, -1, vb,
+                                      dv, yoff);
+                jb = first_at_or_past(jlo, jhi, (yb - vb) * inv_dv, -1, -1, vb, dv, yoff) - 1;
+              }
+              // A guard-band sample just outside a y face of the grid has its
+              // cell row clamped into the edge tile by the guard-band pass; the
+              // fast loop does not see it, so the row asks for that pass here.
+              // Only the samples next to [ja, jb] (or the ends of an empty run)
+              // can lie within the guard band of a face: cell rows are
+              // monotone in j and |dv| < 1/2.
+              const int c1 = ja <= jb ? ja - 1 : jlo, c2 = ja <= jb ? jb + 1 : jhi;
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int jc = e ? c2 : c1;
+                if (jc < jlo || jc > jhi) continue;
+                const SampleC cc = classify(fma2(pk2((float)jc, (float)jc), pk2(du, dv),
+                                                 pk2(ub, vb)),
+                                            magic2, half2, halfband);
+                float csx, csy;
+                upk2(cc.s, csx, csy);
+                const int cy = min(max(__float_as_int(csy) - kMagicBits + C, 0), W - 1) - y0;
+                edge |= cc.band & ((unsigned)cy < (unsigned)H);
+              }
+            }
           }
-          // ---- the non-empty rows, longest first (rows walked together then
-          // have similar lengths), kGroup at a time
-          const bool live_row = valid && jlo <= jhi;
+          // ---- rows with fast samples or guard-band work, longest fast run
+          // first (rows walked together then have similar lengths), kGroup at
+          // a time
+          const bool live_row = valid && jlo <= jhi && (ja <= jb || zexact || edge);
           const int nrows = __popc(__ballot_sync(kFull, live_row));
           if (live_row) {
+            // i, j in [-L, L) fit 16 bits (L <= 8 n and n < 3600 for a staged tile)
             float4 *rec = s_rows[warp][lane];
-            rec[0] = make_float4(ub, vb, tz, __int_as_float(jlo));
-            rec[1] = make_float4(__int_as_float(jhi), __int_as_float(is), __int_as_float(i),
-                                 __int_as_float((int)zexact));
+            rec[0] = make_float4(ub, vb, tz, __int_as_float(ja));
+            rec[1] = make_float4(
+                __int_as_float(jb), __int_as_float(is),
+                __int_as_float((int)(((unsigned)i << 16) | ((unsigned)jlo & 0xFFFFu))),
+                __int_as_float((int)(((unsigned)jhi << 16) | (unsigned)zexact |
+                                     ((unsigned)edge << 1))));
           }
-          // bitonic sort of (length, lane) keys, descending; empty rows last
-          unsigned key = live_row ? ((unsigned)(jhi - jlo + 1) << 5) | (unsigned)lane : 0u;
+          // bitonic sort of (fast length, lane) keys, descending; empty slots last
+          unsigned key =
+              live_row ? ((unsigned)(max(jb - ja + 1, 0) + 1) << 5) | (unsigned)lane : 0u;
 #pragma unroll
           for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
@@ -418,34 +496,42 @@ __global__ void __launch_bounds__(kThreads, 1)
             const float4 r0v = rec[0], r1v = rec[1];
             const float k_ubm = r0v.x, k_vbm = r0v.y;  // q - 1/2 at j = 0
             const float k_tz = r0v.z;
-            const int k_jlo = __float_as_int(r0v.w);
-            const int k_jhi = rvalid ? __float_as_int(r1v.x) : k_jlo - 1;
-            const int k_is = __float_as_int(r1v.y), k_i = __float_as_int(r1v.z);
-            const bool k_zx = rvalid && __float_as_int(r1v.w) != 0;
+            const int k_ja = __float_as_int(r0v.w);
+            const int k_jb = rvalid ? __float_as_int(r1v.x) : k_ja - 1;
+            const int k_is = __float_as_int(r1v.y);
+            const int k_pz = __float_as_int(r1v.z), k_pw = __float_as_int(r1v.w);
+            const int k_i = k_pz >> 16, k_jlo = (int)(short)(k_pz & 0xFFFF);
+            const int k_jhi = rvalid ? (k_pw >> 16) : k_jlo - 1;
+            const bool k_zx = rvalid && (k_pw & 1) != 0;
+            const bool k_edge = rvalid && (k_pw & 2) != 0;
             const u64 qb = pk2(k_ubm, k_vbm), tz2 = pk2(k_tz, k_tz);
-            const int len = k_jhi - k_jlo + 1;
+            const int len = k_jb - k_ja + 1;
             const int trips = (int)__reduce_max_sync(
                 kFull, (unsigned)((max(len, 0) + kLanesPerRow - 1) / kLanesPerRow));
-            const float jhif = (float)k_jhi;
-            const float jf0 = (float)(k_jlo + pos);
-            bool any_band = k_zx;
+            const float jbf = (float)k_jb;
+            const float jf0 = (float)(k_ja + pos);
+            bool any_band = k_zx | k_edge;
             float part = 0.0f;
             {
-              // a row in the z band has no fast samples: its last fast j is jlo - 1
-              const float jhif_fast = k_zx ? jf0 - 1.0f : jhif;
               u64 jj = pk2(jf0, jf0);
-#pragma unroll 2
+#pragma unroll 4
               for (int t = 0; t < trips; ++t, jj = add2(jj, step2)) {
                 float jf, jf_hi;
                 upk2(jj, jf, jf_hi);
                 const SampleC c = classify(fma2(jj, duv, qb), magic2, half2, halfband);
                 float sx, sy;
                 upk2(c.s, sx, sy);
-                const int iyr = __float_as_int(sy) - yoff;
-                const bool live = jf <= jhif_fast;
+                const bool live = jf <= jbf;  // in [ja, jb]: cell row in the tile
                 any_band |= live & c.band;
-                if (live & !c.band & ((unsigned)iyr < (unsigned)H)) {
-                  const unsigned a = sbase + 16u * (unsigned)(iyr * qp + __float_as_int(sx));
+                const bool fast = live & !c.band;
+                {
+                  // branch-free: a lane without a fast sample reads the zero
+                  // quads of the padding column (staged column 0, node rows 0
+                  // and 1) and adds 0
+                  const unsigned a =
+                      fast ? (unsigned)__float_as_int(sy) * qp16 +
+                                 ((unsigned)__float_as_int(sx) << 4) + abase
+                           : smem0;
                   u64 a01, a23, b01, b23;
                   lds_pairs(a, a01, a23);
                   lds_pairs(a + qp16, b01, b23);
@@ -455,15 +541,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                   upk2(c.t, tx, ty);
                   const float va = fmaf(tx, cxa, ca), vb2 = fmaf(tx, cxb, cb);
                   part += fmaf(ty, vb2 - va, va);
-                  if (kCount) ++evaluated;
+                  if (kCount) evaluated += fast;
                 }
               }
             }
             // ---- guard-band samples (and whole rows in the z band) go to the
             // warp's queue; full warps of them take the FP64 path below
             if (__any_sync(kFull, any_band)) {
-              u64 jj = pk2(jf0, jf0);
-              for (int t = 0; t < trips; ++t, jj = add2(jj, step2)) {
+              // walks the row's whole candidate range [jlo, jhi]
+              const int blen = k_jhi - k_jlo + 1;
+              const int btrips = (int)__reduce_max_sync(
+                  kFull, (unsigned)((max(blen, 0) + kLanesPerRow - 1) / kLanesPerRow));
+              const float jhif = (float)k_jhi;
+              const float bj0 = (float)(k_jlo + pos);
+              u64 jj = pk2(bj0, bj0);
+              for (int t = 0; t < btrips; ++t, jj = add2(jj, step2)) {
                 float jf, jf_hi;
                 upk2(jj, jf, jf_hi);
                 const SampleC c = classify(fma2(jj, duv, qb), magic2, half2, halfband);
