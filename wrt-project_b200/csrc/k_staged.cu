@@ -94,10 +94,6 @@ __device__ __forceinline__ double ldsd(const double *p) {
   asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
   return v;
 }
-// 16-byte shared-memory load as two pairs, 32-bit shared address
-__device__ __forceinline__ void lds_pairs(unsigned addr, u64 &lo, u64 &hi) {
-  asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(lo), "=l"(hi) : "r"(addr));
-}
 
 // z cell coordinate of lattice row i of (shift s, direction): w = (s nz + i
 // delta v1z + 1) h, in FP64 with explicit roundings (the same value wherever
@@ -211,6 +207,74 @@ __device__ __forceinline__ SampleC classify(u64 q, u64 magic2, u64 half2, float 
   c.band = fmaxf(fabsf(dx), fabsf(dy)) > halfband;
   return c;
 }
+
+// One sample of the fast loop, written in PTX so that it compiles to the
+// instructions it names (the same computation in C++ came out ~8 instructions
+// longer per sample): position q = j (du, dv) + qb, the classification of
+// classify() bit for bit, the guard-band and row-end tests as predicates, the
+// shared address (bits(y' + magic) * 16 qp + 16 bits(x' + magic) + abase, or
+// the zero padding quad when the sample is not a fast one), two 16-byte loads
+// (node rows y, y+1), the z-lerp of both quad halves as pairs, the x- and
+// y-lerps, the running sum.  anyb |= 1 for a guard-band sample in the row;
+// cnt counts fast samples (measurement build).
+#define WRT_SAMPLE_STEP_PTX(COUNT_LINE)                                              \
+  "{\n\t"                                                                            \
+  ".reg .b64 q, s, r, d, t, a01, a23, b01, b23, za, zb;\n\t"                         \
+  ".reg .f32 dx, dy, m, jf, jfh, tx, ty, ca, cxa, cb, cxb, va, vb, df;\n\t"          \
+  ".reg .b32 sxb, syb, addr, addr2, ax;\n\t"                                         \
+  ".reg .pred live, band, fast;\n\t"                                                 \
+  "fma.rn.f32x2 q, %3, %4, %5;\n\t"                                                  \
+  "add.rn.f32x2 s, q, %6;\n\t"                                                       \
+  "sub.rn.f32x2 r, s, %6;\n\t"                                                       \
+  "sub.rn.f32x2 d, q, r;\n\t"                                                        \
+  "add.rn.f32x2 t, d, %7;\n\t"                                                       \
+  "mov.b64 {dx, dy}, d;\n\t"                                                         \
+  "abs.f32 dx, dx;\n\t"                                                              \
+  "abs.f32 dy, dy;\n\t"                                                              \
+  "max.f32 m, dx, dy;\n\t"                                                           \
+  "mov.b64 {jf, jfh}, %3;\n\t"                                                       \
+  "setp.le.f32 live, jf, %9;\n\t"                                                    \
+  "setp.gt.and.f32 band, m, %8, live;\n\t"                                           \
+  "setp.le.and.f32 fast, m, %8, live;\n\t"                                           \
+  "@band or.b32 %1, %1, 1;\n\t"                                                      \
+  COUNT_LINE                                                                         \
+  "mov.b64 {sxb, syb}, s;\n\t"                                                       \
+  "shl.b32 ax, sxb, 4;\n\t"                                                          \
+  "mad.lo.u32 addr, syb, %10, %11;\n\t"                                              \
+  "add.u32 addr, addr, ax;\n\t"                                                      \
+  "selp.b32 addr, addr, %12, fast;\n\t"                                              \
+  "add.u32 addr2, addr, %10;\n\t"                                                    \
+  "ld.shared.v2.b64 {a01, a23}, [addr];\n\t"                                         \
+  "ld.shared.v2.b64 {b01, b23}, [addr2];\n\t"                                        \
+  "fma.rn.f32x2 za, a23, %13, a01;\n\t"                                              \
+  "fma.rn.f32x2 zb, b23, %13, b01;\n\t"                                              \
+  "mov.b64 {ca, cxa}, za;\n\t"                                                       \
+  "mov.b64 {cb, cxb}, zb;\n\t"                                                       \
+  "mov.b64 {tx, ty}, t;\n\t"                                                         \
+  "fma.rn.f32 va, tx, cxa, ca;\n\t"                                                  \
+  "fma.rn.f32 vb, tx, cxb, cb;\n\t"                                                  \
+  "sub.rn.f32 df, vb, va;\n\t"                                                       \
+  "fma.rn.f32 va, ty, df, va;\n\t"                                                   \
+  "add.rn.f32 %0, %0, va;\n\t"                                                       \
+  "}"
+
+template <bool kCount>
+__device__ __forceinline__ void sample_step(u64 jj, u64 duv, u64 qb, u64 magic2, u64 half2,
+                                            float halfband, float jbf, unsigned qp16,
+                                            unsigned abase, unsigned zaddr, u64 tz2,
+                                            float &part, unsigned &anyb, unsigned &cnt) {
+  if (kCount)
+    asm(WRT_SAMPLE_STEP_PTX("@fast add.u32 %2, %2, 1;\n\t")
+        : "+f"(part), "+r"(anyb), "+r"(cnt)
+        : "l"(jj), "l"(duv), "l"(qb), "l"(magic2), "l"(half2), "f"(halfband), "f"(jbf),
+          "r"(qp16), "r"(abase), "r"(zaddr), "l"(tz2));
+  else
+    asm(WRT_SAMPLE_STEP_PTX("")
+        : "+f"(part), "+r"(anyb), "+r"(cnt)
+        : "l"(jj), "l"(duv), "l"(qb), "l"(magic2), "l"(half2), "f"(halfband), "f"(jbf),
+          "r"(qp16), "r"(abase), "r"(zaddr), "l"(tz2));
+}
+#undef WRT_SAMPLE_STEP_PTX
 
 // FP64 reference evaluation of `count` queued guard-band samples of direction
 // d, one per lane, each added to its plane as a fixed-point integer.  Returns
@@ -513,37 +577,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool any_band = k_zx | k_edge;
             float part = 0.0f;
             {
+              // branch-free: a lane past its row's end or on a guard-band
+              // sample reads the zero quads of the padding column (staged
+              // column 0, node rows 0 and 1) and adds 0
+              unsigned anyb = 0, cnt = 0;
               u64 jj = pk2(jf0, jf0);
 #pragma unroll 4
-              for (int t = 0; t < trips; ++t, jj = add2(jj, step2)) {
-                float jf, jf_hi;
-                upk2(jj, jf, jf_hi);
-                const SampleC c = classify(fma2(jj, duv, qb), magic2, half2, halfband);
-                float sx, sy;
-                upk2(c.s, sx, sy);
-                const bool live = jf <= jbf;  // in [ja, jb]: cell row in the tile
-                any_band |= live & c.band;
-                const bool fast = live & !c.band;
-                {
-                  // branch-free: a lane without a fast sample reads the zero
-                  // quads of the padding column (staged column 0, node rows 0
-                  // and 1) and adds 0
-                  const unsigned a =
-                      fast ? (unsigned)__float_as_int(sy) * qp16 +
-                                 ((unsigned)__float_as_int(sx) << 4) + abase
-                           : smem0;
-                  u64 a01, a23, b01, b23;
-                  lds_pairs(a, a01, a23);
-                  lds_pairs(a + qp16, b01, b23);
-                  float ca, cxa, cb, cxb, tx, ty;
-                  upk2(fma2(a23, tz2, a01), ca, cxa);  // (v + tz dz, dv/dx + tz d(dz)/dx)
-                  upk2(fma2(b23, tz2, b01), cb, cxb);
-                  upk2(c.t, tx, ty);
-                  const float va = fmaf(tx, cxa, ca), vb2 = fmaf(tx, cxb, cb);
-                  part += fmaf(ty, vb2 - va, va);
-                  if (kCount) evaluated += fast;
-                }
-              }
+              for (int t = 0; t < trips; ++t, jj = add2(jj, step2))
+                sample_step<kCount>(jj, duv, qb, magic2, half2, halfband, jbf, qp16, abase, smem0,
+                                    tz2, part, anyb, cnt);
+              any_band |= anyb != 0;
+              if (kCount) evaluated += cnt;
             }
             // ---- guard-band samples (and whole rows in the z band) go to the
             // warp's queue; full warps of them take the FP64 path below
