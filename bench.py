@@ -497,6 +497,116 @@ def run_ours(args, dist):
     return 0
 
 
+# ------------------------------------------------------------ other paths
+PATHS = {
+    # path: (metric, unit, workload)
+    "ray": ("rays/s @128^3 (128 layers x 128 shifts x 128 angles, reference frame)", "rays/s",
+            "ray_grid, 128^3 volume of 16 seeded ellipsoids, 128 z-layers x 128 shifts x 128 "
+            "angles, trilinear, 513 samples per ray (255 inside the unit ball)"),
+    "reduction": ("plane integrals/s from 128^3 ray data (64x128 sphere grid x 256 shifts)",
+                  "plane integrals/s",
+                  "radon_reduction, rays 128 layers x 128 shifts x 128 angles -> 64x128 sphere "
+                  "grid x 256 shifts (ray shift grid decoupled: spline over 128 offsets)"),
+    "adjoint": ("voxels/s of the backprojection to 128^3 (64x128 sphere grid x 256 shifts)",
+                "voxels/s",
+                "radon3d_adjoint, seeded N(0,1) Radon data 64x128 sphere grid x 256 shifts -> "
+                "128^3 voxels, 8192 spline evaluations per voxel"),
+}
+
+
+def run_path(args, dist):
+    """One of the other hot paths through its drop-in entry point (host arrays
+    in and out, as the reference's programs take them): K timed calls after W
+    warm-up calls, CUDA events on the library's stream around each call (the
+    calls are synchronous, so this is end to end), the reference's own code on
+    a bounded sample of the same workload on the host cores beside it."""
+    wrt = load_package()
+    from wrt_b200.phantom import ellipsoid_phantom
+
+    sys.path.insert(0, str(ROOT))
+    import oracle as O
+
+    metric, unit, workload = PATHS[args.path]
+    ctx = wrt.Context(dist.local_rank)
+    n = N
+    rng = np.random.default_rng(SEED)
+    vol = ellipsoid_phantom(n, ELLIPSOIDS, SEED)
+    if args.path == "ray":
+        call = lambda: ctx.ray_grid(vol, n, 128, 128)
+        units, h2d, d2h = n * 128 * 128, vol.nbytes, n * 128 * 128 * 8
+    elif args.path == "reduction":
+        rays = ctx.ray_grid(vol, n, 128, 128)
+        call = lambda: ctx.radon_reduction(rays, NSHIFT, NTHETA)
+        units, h2d, d2h = NSHIFT * NPHI * NTHETA, rays.nbytes, NSHIFT * NPHI * NTHETA * 8
+    else:
+        radon = rng.standard_normal((NSHIFT, NPHI, NTHETA))
+        call = lambda: ctx.radon3d_adjoint(radon, n)
+        units, h2d, d2h = n ** 3, radon.nbytes, n ** 3 * 8
+    for _ in range(max(args.warmup, 3)):
+        result = call()
+    ctx.synchronize()
+    clocks = ClockSampler(dist.local_rank)
+    clocks.start()
+    dist.barrier()
+    times = []
+    for _ in range(args.steps):
+        ctx.timer_start()
+        result = call()
+        times.append(ctx.timer_stop())
+    dist.barrier()
+    clk = clocks.stop()
+    total_ms = dist.max(sum(times))
+    value = units * args.steps * dist.world / (total_ms * 1e-3)
+
+    # the reference on the host cores: a bounded seeded sample of the same units
+    cpu = None
+    if dist.rank == 0 and not args.no_cpu_baseline and O.Reference.available():
+        ref, cores = O.Reference(), cpu_threads()
+        t0 = time.perf_counter()
+        if args.path == "ray":
+            m = 65536
+            idx = rng.integers(0, units, size=m)
+            s_grid, phi_grid = O.ray_grid(128, 128)
+            z = -1.0 + (idx // (128 * 128)) * (2.0 / (n - 1))
+            got = ref.rays(vol, z, s_grid[(idx // 128) % 128], phi_grid[idx % 128], cores)
+            ours = result.reshape(-1)[idx]
+        elif args.path == "reduction":
+            m = 4096
+            idx = rng.integers(0, units, size=m)
+            # the reference couples the ray and Radon shift grids: rays on 256 shifts
+            rays_c = ctx.ray_grid(vol, n, NSHIFT, 128)
+            t0 = time.perf_counter()
+            got = ref.reduction_planes(rays_c, NTHETA, idx // (NPHI * NTHETA),
+                                       (idx // NTHETA) % NPHI, idx % NTHETA, cores)
+            ours = None
+        else:
+            m = 64
+            idx = rng.integers(0, units, size=m)
+            iz, ix, iy = idx // (n * n), (idx // n) % n, idx % n
+            c = lambda i: -1.0 + (2.0 * i + 1.0) / n
+            got = ref.adjoint_points(radon, c(ix), c(iy), c(iz), cores)
+            ours = result.reshape(-1)[idx]
+        wall = time.perf_counter() - t0
+        cpu = {"value": m / wall, "unit": unit, "cores": cores, "kind": "reference",
+               "sample": f"{m} seeded random units of this workload, the reference's own code "
+                         "(oracle/_ref) with OpenMP over units"}
+        if ours is not None:
+            cpu["rel_l2_gpu_vs_reference_on_sample"] = float(
+                np.linalg.norm(ours - got) / max(np.linalg.norm(got), 1e-300))
+    if dist.rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": unit, "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "path": args.path,
+            "config": {"workload": workload, "api": "drop-in entry point, host arrays"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "clocks": clk, "cpu_baseline": cpu}))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,6 +622,9 @@ def main():
                     help="requests in the mixed serving stream")
     ap.add_argument("--tile", type=int, default=None,
                     help="use this tile configuration of the staged kernel instead of tuning")
+    ap.add_argument("--path", choices=["forward", *PATHS], default="forward",
+                    help="forward: the headline (plane integrals at 128^3); ray, reduction, "
+                         "adjoint: the other hot paths through their drop-in entry points")
     ap.add_argument("--grid", default=None,
                     help="NPHI,NTHETA,NSHIFT: a smaller sphere grid (profiling captures only)")
     args = ap.parse_args()
@@ -520,7 +633,10 @@ def main():
         NPHI, NTHETA, NSHIFT = (int(x) for x in args.grid.split(","))
     dist = Dist(args.gpus)
     try:
-        rc = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if args.path != "forward":
+            rc = run_path(args, dist) if args.impl == "ours" else 0
+        else:
+            rc = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
     finally:
         dist.close()
     return rc
