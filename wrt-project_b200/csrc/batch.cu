@@ -164,10 +164,9 @@ __global__ void __launch_bounds__(256) batch_adjoint_kernel(const char *t) {
   const long long nth = (long long)gridDim.x * blockDim.x;
   for (int r = 0; r < na; ++r) {
     const int n = J[r].n;
-    const long long total = (long long)n * n * n;
-    for (long long k = tid; k < total; k += nth)
-      J[r].out[k] = wrtd::adjoint_voxel(J[r].lines, J[r].ndir, J[r].ntheta, J[r].nshift,
-                                        J[r].dirw, n, k);
+    const long long items = wrtd::adjoint_items(n);
+    for (long long t2 = tid; t2 < items; t2 += nth)
+      wrtd::adjoint_item(J[r].lines, J[r].ndir, J[r].nshift, J[r].dirw, n, t2, J[r].out);
   }
 }
 

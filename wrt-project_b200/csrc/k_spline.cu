@@ -89,15 +89,15 @@ __global__ void __launch_bounds__(256)
   out[k] = acc * dtau;
 }
 
-// Adjoint: one thread per voxel, output order [iz][ix][iy]; loop over all
-// directions.  dirw[d] = (sin t cos p, sin t sin p, cos t, dphi * w_t).
+// Adjoint: one thread per wrtd::kAdjVoxels voxels along x, output order
+// [iz][ix][iy]; loop over all directions.  dirw[d] = (sin t cos p,
+// sin t sin p, cos t, dphi * w_t).
 __global__ void __launch_bounds__(256)
-    adjoint_kernel(const float4 *__restrict__ lines /* [d][ns-1] */, int ndir, int ntheta, int ns,
+    adjoint_kernel(const float4 *__restrict__ lines /* [d][ns-1] */, int ndir, int ns,
                    const double4 *__restrict__ dirw, int n, double *__restrict__ out) {
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long total = (long long)n * n * n;
-  if (k >= total) return;
-  out[k] = wrtd::adjoint_voxel(lines, ndir, ntheta, ns, dirw, n, k);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= wrtd::adjoint_items(n)) return;
+  wrtd::adjoint_item(lines, ndir, ns, dirw, n, t, out);
 }
 
 int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long long so,
@@ -165,9 +165,10 @@ int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, i
 
 int launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int ntheta, int nshift,
                    const double4 *d_dirw, int n, double *d_out) {
-  const long long total = (long long)n * n * n;
-  adjoint_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_lines, ndir, ntheta,
-                                                                        nshift, d_dirw, n, d_out);
+  (void)ntheta;
+  const long long items = wrtd::adjoint_items(n);
+  adjoint_kernel<<<(unsigned)((items + 255) / 256), 256, 0, stream>>>(d_lines, ndir, nshift,
+                                                                        d_dirw, n, d_out);
   return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
 }
 
@@ -202,9 +203,9 @@ int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, i
   const int ndir = nphi * ntheta;
   int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, &bytes);
   if (st) return st;
-  const long long total = (long long)n * n * n;
-  adjoint_kernel<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(
-      d_lines, ndir, ntheta, nshift, d_dirw, n, d_out);
+  const long long items = wrtd::adjoint_items(n);
+  adjoint_kernel<<<(unsigned)((items + 255) / 256), 256, 0, ctx->stream>>>(
+      d_lines, ndir, nshift, d_dirw, n, d_out);
   ctx->launches++;
   st = check_launch(ctx, "adjoint_kernel");
   if (!st) {

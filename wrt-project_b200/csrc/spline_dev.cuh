@@ -59,47 +59,60 @@ __device__ __forceinline__ float spline_eval(const float4 *__restrict__ line, in
   return fmaf(a, c.x, b * c.y) + ((a * a - 1.0f) * a * c.z + (b * b - 1.0f) * b * c.w) * h2_6;
 }
 
-// Backprojection of one voxel k (output order [iz][ix][iy], cell centres,
-// radon_inversion/backprojection/C/src/radon3d_ajoint.c:240-254):
-//   sum over directions d of dphi*w_theta * S_d(<x, omega_d>), S_d = 0 beyond |s| > 1
-// (backprojection/C/src/integral.c:6-24).  The plane coordinate s = <x, omega>
-// and its knot position are FP64 (dirw holds the reference's FP64 omega); the
-// spline value and the weighted sum are FP32, compensated (Kahan) per latitude
-// ring, FP64 over rings: Radon data of mixed signs cancel strongly in this
-// sum, and a plain FP32 accumulator would lose up to ~1e-5 of the result.
-__device__ __forceinline__ double adjoint_voxel(const float4 *__restrict__ lines, int ndir,
-                                                int ntheta, int ns,
-                                                const double4 *__restrict__ dirw, int n,
-                                                long long k) {
-  const int iy = (int)(k % n), ix = (int)((k / n) % n), iz = (int)(k / ((long long)n * n));
-  const double x = (-1.0) + (1.0 / n) + ix * (2.0 / n);
+// Backprojection (radon_inversion/backprojection/C/src/integral.c:6-24,
+// output order [iz][ix][iy] at cell centres, radon3d_ajoint.c:240-254):
+//   R*g(x) = sum over directions d of dphi*w_theta * S_d(<x, omega_d>), S_d = 0
+//   beyond |s| > 1.
+// One thread takes kAdjVoxels voxels along x, (iz, ix0 + v, iy): per direction
+// it reads dirw once and steps the knot position q = (s + 1)/h from voxel to
+// voxel by one FP64 add, q and its fraction in FP64 (dirw holds the
+// reference's FP64 omega; a few FP64 roundings from the direct dot product,
+// 1e-14 knots at most), the spline value and its weight in FP32, the sum over
+// directions in FP64.  |s| <= 1 is tested as 0 <= q <= ns - 1.  Threads of a
+// warp take consecutive iy: one direction's 32 lanes read neighbouring knot
+// intervals of one line.
+constexpr int kAdjVoxels = 4;
+
+// thread items of an n^3 adjoint: (iz, ix group, iy), iy fastest
+__host__ __device__ inline long long adjoint_items(int n) {
+  return (long long)n * n * ((n + kAdjVoxels - 1) / kAdjVoxels);
+}
+
+__device__ __forceinline__ void adjoint_item(const float4 *__restrict__ lines, int ndir, int ns,
+                                             const double4 *__restrict__ dirw, int n,
+                                             long long t, double *__restrict__ out) {
+  const int ngx = (n + kAdjVoxels - 1) / kAdjVoxels;
+  const int iy = (int)(t % n), ix0 = (int)((t / n) % ngx) * kAdjVoxels,
+            iz = (int)(t / ((long long)n * ngx));
+  const double x0 = (-1.0) + (1.0 / n) + ix0 * (2.0 / n);
   const double y = (-1.0) + (1.0 / n) + iy * (2.0 / n);
   const double z = (-1.0) + (1.0 / n) + iz * (2.0 / n);
   const float hs = 2.0f / (float)(ns - 1);
-  const double inv_hs = 0.5 * (double)(ns - 1);
+  const double inv_hs = 0.5 * (double)(ns - 1), qmax = (double)(ns - 1);
+  const double qdx = (2.0 / n) * inv_hs;  // knot step per voxel along x, per unit omega_x
   const float h2_6 = hs * hs / 6.0f;
   const size_t line_len = (size_t)(ns - 1);
-  double acc = 0.0;
-  for (int d0 = 0; d0 < ndir; d0 += ntheta) {
-    float part = 0.0f, comp = 0.0f;  // running sum and its lost low-order part
-    const int d1 = min(ndir, d0 + ntheta);
-    for (int d = d0; d < d1; ++d) {
-      const double2 w01 = __ldg(reinterpret_cast<const double2 *>(dirw + d));
-      const double2 w23 = __ldg(reinterpret_cast<const double2 *>(dirw + d) + 1);
-      const double4 w = make_double4(w01.x, w01.y, w23.x, w23.y);
-      const double s = fma(x, w.x, fma(y, w.y, z * w.z));
-      if (fabs(s) <= 1.0) {
-        const float term = __fmul_rn(
-            (float)w.w, spline_eval_q64(lines + d * line_len, ns, fma(s, inv_hs, inv_hs), h2_6));
-        const float yk = __fsub_rn(term, comp);
-        const float t = __fadd_rn(part, yk);
-        comp = __fsub_rn(__fsub_rn(t, part), yk);
-        part = t;
-      }
+  double acc[kAdjVoxels];
+#pragma unroll
+  for (int v = 0; v < kAdjVoxels; ++v) acc[v] = 0.0;
+  for (int d = 0; d < ndir; ++d) {
+    const double2 w01 = __ldg(reinterpret_cast<const double2 *>(dirw + d));
+    const double2 w23 = __ldg(reinterpret_cast<const double2 *>(dirw + d) + 1);
+    const float wf = (float)w23.y;
+    const double q0 = fma(fma(x0, w01.x, fma(y, w01.y, z * w23.x)), inv_hs, inv_hs);
+    const double qs = qdx * w01.x;
+    const float4 *line = lines + d * line_len;
+#pragma unroll
+    for (int v = 0; v < kAdjVoxels; ++v) {
+      const double q = fma((double)v, qs, q0);
+      if (q >= 0.0 && q <= qmax)
+        acc[v] += (double)__fmul_rn(wf, spline_eval_q64(line, ns, q, h2_6));
     }
-    acc += (double)part - (double)comp;
   }
-  return acc;
+  const size_t base = ((size_t)iz * n + ix0) * n + iy;
+#pragma unroll
+  for (int v = 0; v < kAdjVoxels; ++v)
+    if (ix0 + v < n) out[base + (size_t)v * n] = acc[v];
 }
 
 }  // namespace wrtd
