@@ -36,16 +36,15 @@ __device__ __forceinline__ void spline_line(const double *__restrict__ y, long l
     o[i] = make_float4((float)y[i * se], (float)y[(i + 1) * se], (float)M[i], (float)M[i + 1]);
 }
 
-// The same at a knot position q given in FP64 (fraction taken in FP64, then
-// rounded once): for rough data the spline is steep, and an FP32 position
-// error of 1e-7 * (ns - 1) knots would move the value by that much times the
-// slope.
+// The same at a knot position q given in FP64, 0 <= q <= ns - 1 (the
+// caller's range test): fraction taken in FP64, then rounded once.  For rough
+// data the spline is steep, and an FP32 position error of 1e-7 * (ns - 1)
+// knots would move the value by that much times the slope.
 __device__ __forceinline__ float spline_eval_q64(const float4 *__restrict__ line, int ns,
                                                  double q, float h2_6) {
-  double fi = floor(q);
-  fi = fmin(fmax(fi, 0.0), (double)(ns - 2));
-  const float b = (float)(q - fi), a = 1.0f - b;
-  const float4 c = __ldg(line + (int)fi);
+  const int i = min(__double2int_rz(q), ns - 2);  // floor (q >= 0); q = ns - 1: b = 1
+  const float b = (float)(q - (double)i), a = 1.0f - b;
+  const float4 c = __ldg(line + i);
   return fmaf(a, c.x, b * c.y) + ((a * a - 1.0f) * a * c.z + (b * b - 1.0f) * b * c.w) * h2_6;
 }
 
