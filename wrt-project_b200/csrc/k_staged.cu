@@ -304,9 +304,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   // dynamic shared memory: per warp a row table and a guard-band queue, then
   // the staged tile
   extern __shared__ float4 dyn_smem[];
-  // the warp's compacted non-empty rows: (q0x, q0y, tz, jlo) and (jhi, shift
-  // index, i, whole row in the z band)
-  float4(*s_rows)[32][2] = reinterpret_cast<float4(*)[32][2]>(dyn_smem);
+  // the warp's rows: [0][slot] = (q0x, q0y, tz, ja), [1][slot] = (jb, shift
+  // index, i | jlo, jhi | flags); the two halves apart, so that a half-warp's
+  // 4 rows read words that fall in any of the 8 bank groups
+  float4(*s_rows)[2][32] = reinterpret_cast<float4(*)[2][32]>(dyn_smem);
   // guard-band samples waiting for the FP64 path: (shift index, i << 16 | j)
   int2(*s_xq)[64] = reinterpret_cast<int2(*)[64]>(dyn_smem + kWarps * 64);
   float4 *quads = dyn_smem + kWarps * wrt::kStagedWarpSmemQuads;
@@ -531,9 +532,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int nrows = __popc(__ballot_sync(kFull, live_row));
           if (live_row) {
             // i, j in [-L, L) fit 16 bits (L <= 8 n and n < 3600 for a staged tile)
-            float4 *rec = s_rows[warp][lane];
-            rec[0] = make_float4(ub, vb, tz, __int_as_float(ja));
-            rec[1] = make_float4(
+            s_rows[warp][0][lane] = make_float4(ub, vb, tz, __int_as_float(ja));
+            s_rows[warp][1][lane] = make_float4(
                 __int_as_float(jb), __int_as_float(is),
                 __int_as_float((int)(((unsigned)i << 16) | ((unsigned)jlo & 0xFFFFu))),
                 __int_as_float((int)(((unsigned)jhi << 16) | (unsigned)zexact |
@@ -556,8 +556,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int kr = g0 + lane / kLanesPerRow;
             const bool rvalid = kr < nrows;
             const int slot = (int)(__shfl_sync(kFull, key, rvalid ? kr : 0) & 31u);
-            const float4 *rec = s_rows[warp][slot];
-            const float4 r0v = rec[0], r1v = rec[1];
+            const float4 r0v = s_rows[warp][0][slot], r1v = s_rows[warp][1][slot];
             const float k_ubm = r0v.x, k_vbm = r0v.y;  // q - 1/2 at j = 0
             const float k_tz = r0v.z;
             const int k_ja = __float_as_int(r0v.w);
