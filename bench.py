@@ -503,6 +503,11 @@ PATHS = {
     "ray": ("rays/s @128^3 (128 layers x 128 shifts x 128 angles, reference frame)", "rays/s",
             "ray_grid, 128^3 volume of 16 seeded ellipsoids, 128 z-layers x 128 shifts x 128 "
             "angles, trilinear, 513 samples per ray (255 inside the unit ball)"),
+    "ray_rotated": ("rays/s @128^3 (128 layers x 128 shifts x 128 angles, rotated frame)",
+                    "rays/s",
+                    "ray_grid in one seeded random rotation of the layer frame (one of the "
+                    "configuration's orientations), 128^3 volume, 128 layers x 128 shifts x 128 "
+                    "angles, trilinear"),
     "reduction": ("plane integrals/s from 128^3 ray data (64x128 sphere grid x 256 shifts)",
                   "plane integrals/s",
                   "radon_reduction, rays 128 layers x 128 shifts x 128 angles -> 64x128 sphere "
@@ -531,8 +536,14 @@ def run_path(args, dist):
     n = N
     rng = np.random.default_rng(SEED)
     vol = ellipsoid_phantom(n, ELLIPSOIDS, SEED)
-    if args.path == "ray":
-        call = lambda: ctx.ray_grid(vol, n, 128, 128)
+    frame = None
+    if args.path == "ray_rotated":
+        q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+        frame = q * np.sign(np.diag(r))
+        if np.linalg.det(frame) < 0:
+            frame[:, 0] = -frame[:, 0]
+    if args.path in ("ray", "ray_rotated"):
+        call = lambda: ctx.ray_grid(vol, n, 128, 128, frame=frame)
         units, h2d, d2h = n * 128 * 128, vol.nbytes, n * 128 * 128 * 8
     elif args.path == "reduction":
         rays = ctx.ray_grid(vol, n, 128, 128)
@@ -570,6 +581,11 @@ def run_path(args, dist):
             z = -1.0 + (idx // (128 * 128)) * (2.0 / (n - 1))
             got = ref.rays(vol, z, s_grid[(idx // 128) % 128], phi_grid[idx % 128], cores)
             ours = result.reshape(-1)[idx]
+        elif args.path == "ray_rotated":
+            # the reference has no layer frames: the FP64 restatement, all rays
+            m = units
+            got = O.ray_forward(vol, n, 128, 128, frame=frame, nthreads=cores).reshape(-1)
+            ours = result.reshape(-1)
         elif args.path == "reduction":
             m = 4096
             idx = rng.integers(0, units, size=m)
@@ -590,6 +606,9 @@ def run_path(args, dist):
         cpu = {"value": m / wall, "unit": unit, "cores": cores, "kind": "reference",
                "sample": f"{m} seeded random units of this workload, the reference's own code "
                          "(oracle/_ref) with OpenMP over units"}
+        if args.path == "ray_rotated":
+            cpu.update(kind="port", sample=f"all {m} rays, the FP64 oracle restatement with the "
+                                           "frame (the reference has no layer frames)")
         if ours is not None:
             cpu["rel_l2_gpu_vs_reference_on_sample"] = float(
                 np.linalg.norm(ours - got) / max(np.linalg.norm(got), 1e-300))

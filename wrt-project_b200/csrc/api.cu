@@ -822,7 +822,13 @@ int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int n, int nslices, int nsh
     job.r2bits = vol->d_stats;
     job.margin = sampler_margin(n, WRT_SAMPLER_TRILINEAR);
     job.out = dout.as<double>();
-    st = ray_forward(ctx, job);
+    // z-slices read one layer pair each: build the volume's layer pairs
+    if (identity) st = volume_ensure_pairs(vol);
+    if (!st && identity) {
+      job.pairs = vol->d_pairs;
+      job.pitch = vol->pitch;
+    }
+    if (!st) st = ray_forward(ctx, job);
   }
   if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "ray_grid result");
   if (vol) wrt_volume_destroy(vol);

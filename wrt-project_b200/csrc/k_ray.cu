@@ -38,6 +38,31 @@ __device__ __forceinline__ double rot_row(const double *F, int r, double x, doub
                    __dmul_rn(F[3 * r + 2], z));
 }
 
+// The 8 corners (x, y, z) .. (x+1, y+1, z+1) of a reference-frame sample:
+// from the layer pairs P[z][y][x] = (v(x,y,z), v(x,y,z+1)) when the volume has
+// them -- a slice reads one z-layer pair, whose rows are contiguous in x, so
+// neighbouring samples share cache lines -- else from the volume v[x][y][z],
+// where a slice uses 2 of the 32 z values of every line it touches.
+struct Corners {
+  const float *vol;
+  const float2 *pairs;
+  int n, pitch;
+  __device__ __forceinline__ void operator()(int ix, int iy, int zc, float c[8]) const {
+    if (pairs) {
+      const float2 *p = pairs + ((size_t)zc * n + iy) * pitch + ix;
+      const float2 a = __ldg(p), b = __ldg(p + pitch), d = __ldg(p + 1), e = __ldg(p + pitch + 1);
+      c[0] = a.x, c[1] = a.y, c[2] = b.x, c[3] = b.y, c[4] = d.x, c[5] = d.y, c[6] = e.x,
+      c[7] = e.y;
+    } else {
+      const float *p = vol + ((size_t)ix * n + iy) * n + zc;
+      const size_t sx = (size_t)n * n;
+      c[0] = __ldg(p), c[1] = __ldg(p + 1), c[2] = __ldg(p + n), c[3] = __ldg(p + n + 1);
+      c[4] = __ldg(p + sx), c[5] = __ldg(p + sx + 1), c[6] = __ldg(p + sx + n);
+      c[7] = __ldg(p + sx + n + 1);
+    }
+  }
+};
+
 template <bool FRAME>
 __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) {
   const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -47,6 +72,7 @@ __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) 
   const int is = (int)((ray / job.nphi) % job.nshift);
   const int iz = (int)(ray / ((long long)job.nphi * job.nshift));
   const int n = job.n;
+  const Corners corners{job.vol, job.pairs, n, job.pitch};
   const double *T = job.trig + 4 * ip;
   const double s = job.shift[is];
   const double dz = 2.0 / (job.nslices - 1);                     // ray_grid.c:244
@@ -143,11 +169,10 @@ __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) 
             // bilinear in x, y on layers zc and zc+1, then the ray's z weight
             const float fx = floorf(qx), fy = floorf(qy);
             const float tx = qx - fx, ty = qy - fy;
-            const float *p = job.vol + ((size_t)(int)fx * n + (int)fy) * n + zc;
-            const size_t sx = (size_t)n * n;
-            const float c000 = __ldg(p), c001 = __ldg(p + 1), c010 = __ldg(p + n),
-                        c011 = __ldg(p + n + 1), c100 = __ldg(p + sx), c101 = __ldg(p + sx + 1),
-                        c110 = __ldg(p + sx + n), c111 = __ldg(p + sx + n + 1);
+            float c[8];
+            corners((int)fx, (int)fy, zc, c);
+            const float c000 = c[0], c001 = c[1], c010 = c[2], c011 = c[3], c100 = c[4],
+                        c101 = c[5], c110 = c[6], c111 = c[7];
             const float a0 = wrtd::lerp32(tx, c000, c100), a1 = wrtd::lerp32(tx, c010, c110);
             const float b0 = wrtd::lerp32(tx, c001, c101), b1 = wrtd::lerp32(tx, c011, c111);
             const float e0 = wrtd::lerp32(ty, a0, a1), e1 = wrtd::lerp32(ty, b0, b1);

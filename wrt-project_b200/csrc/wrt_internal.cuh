@@ -255,6 +255,8 @@ struct RayJob {
   const unsigned int *r2bits;
   double margin;
   double *out;          // [nslices][nshift][nphi]
+  const float2 *pairs;  // layer pairs [n-1][n][pitch] of the volume, or null
+  int pitch;
 };
 int ray_forward(wrt_ctx *ctx, const RayJob &job);
 
