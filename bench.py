@@ -616,6 +616,7 @@ def run_path(args, dist):
         print(json.dumps({
             "metric": metric, "value": value, "unit": unit, "n_gpus": dist.world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "ms_per_step_median": statistics.median(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "path": args.path,
             "config": {"workload": workload, "api": "drop-in entry point, host arrays"},
