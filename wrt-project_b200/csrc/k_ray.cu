@@ -5,8 +5,9 @@
 // sampler.  With a frame F every point is mapped to F p(k) (the layer scheme
 // about another axis; F = identity reproduces the reference).
 //
-// One lane per ray, 32 consecutive rays of the output order [z][s][phi] per
-// warp.  Samples farther than sqrt(crop_r2) from the origin or outside the
+// One lane per ray; a warp takes 32 consecutive shifts of one (z, phi):
+// parallel rays one shift step apart, whose samples read neighbouring cache
+// lines (2.2x faster than 32 angles of one shift, which fan out).  Samples farther than sqrt(crop_r2) from the origin or outside the
 // cube are skipped (their value is exactly 0).  Numerics: FP32 cell
 // coordinates with the guard band of wrt_internal.cuh.  In the reference
 // frame the z coordinate of a ray is one FP64 number for all its samples, so
@@ -68,8 +69,8 @@ __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) 
   const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nrays = (long long)job.nslices * job.nshift * job.nphi;
   if (ray >= nrays) return;
-  const int ip = (int)(ray % job.nphi);
-  const int is = (int)((ray / job.nphi) % job.nshift);
+  const int is = (int)(ray % job.nshift);
+  const int ip = (int)((ray / job.nshift) % job.nphi);
   const int iz = (int)(ray / ((long long)job.nphi * job.nshift));
   const int n = job.n;
   const Corners corners{job.vol, job.pairs, n, job.pitch};
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) 
       acc += (double)part;
     }
   }
-  job.out[ray] = acc * delta;
+  job.out[((long long)iz * job.nshift + is) * job.nphi + ip] = acc * delta;
 }
 
 }  // namespace
