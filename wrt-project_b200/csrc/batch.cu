@@ -152,7 +152,8 @@ __global__ void batch_spline_kernel(const char *t) {
     const int ns = J[r].nshift, nd = J[r].ndir;
     for (long long L = tid; L < nd; L += nth)
       wrtd::spline_line(J[r].radon + L, nd, ns, 2.0 / (ns - 1), J[r].cp, J[r].den,
-                        J[r].scratch + (size_t)L * ns, J[r].lines + (size_t)L * (ns - 1));
+                        J[r].scratch + (size_t)L * ns, J[r].lines + (size_t)L * (ns - 1),
+                        J[r].dirw[L].w);  // the direction's quadrature weight
   }
 }
 

@@ -28,7 +28,7 @@ namespace wrt {
 int launch_gl_nodes(cudaStream_t stream, int n, double *d_x, double *d_w);
 int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
                          const double *d_cp, const double *d_den, double *d_scratch,
-                         float4 *d_lines);
+                         float4 *d_lines, const double4 *d_dirw);
 int launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int ntheta, int nshift,
                    const double4 *d_dirw, int n, double *d_out);
 }  // namespace wrt
@@ -133,7 +133,7 @@ extern "C" int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, i
     direction_weights_kernel<<<(int)((ndir + 127) / 128), 128, 0, s>>>(nphi, ntheta, x, w, dirw);
     st = cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
   }
-  if (!st) st = wrt::launch_adjoint_lines(s, d_radon, (int)ndir, nshift, cp, den, M, lines);
+  if (!st) st = wrt::launch_adjoint_lines(s, d_radon, (int)ndir, nshift, cp, den, M, lines, dirw);
   if (!st) st = wrt::launch_adjoint(s, lines, (int)ndir, ntheta, nshift, dirw, ngrid, d_out);
   ctx->launches += 5;
   if (st) return wrt::fail(ctx, WRT_ERR_CUDA, "radon3d_adjoint_static: launch failed");

@@ -28,12 +28,15 @@ namespace {
 __global__ void spline_prep_kernel(const double *__restrict__ src, int nlines, int ninner,
                                    long long so, long long se, long long si, int ns, double h,
                                    const double *__restrict__ cp, const double *__restrict__ den,
-                                   double *__restrict__ scratch, float4 *__restrict__ out) {
+                                   double *__restrict__ scratch, float4 *__restrict__ out,
+                                   const double4 *__restrict__ weights) {
   const int L = blockIdx.x * blockDim.x + threadIdx.x;
   if (L >= nlines) return;
   const int outer = L / ninner, inner = L % ninner;
+  // adjoint lines carry their direction's quadrature weight dphi * w_theta
+  const double scale = weights ? weights[L].w : 1.0;
   wrtd::spline_line(src + outer * so + inner * si, se, ns, h, cp, den, scratch + (size_t)L * ns,
-                    out + (size_t)L * (ns - 1));
+                    out + (size_t)L * (ns - 1), scale);
 }
 
 // Reduction: one thread per Radon sample (is, iphi, itheta), order of
@@ -101,7 +104,8 @@ __global__ void __launch_bounds__(256)
 }
 
 int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long long so,
-               long long se, long long si, int ns, float4 **d_lines, size_t *bytes) {
+               long long se, long long si, int ns, float4 **d_lines, size_t *bytes,
+               const double4 *d_weights) {
   // line-independent elimination coefficients for the uniform-knot system
   // h M_{i-1} + 4h M_i + h M_{i+1} = rhs (divided by h: M_{i-1} + 4 M_i + M_{i+1})
   const double h = 2.0 / (ns - 1);
@@ -132,7 +136,8 @@ int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long l
       st = wrt::cuda_fail(ctx, e, "spline coefficients");
     } else {
       spline_prep_kernel<<<(nlines + 127) / 128, 128, 0, ctx->stream>>>(
-          d_src, nlines, ninner, so, se, si, ns, h, d_coef, d_coef + ns, d_scratch, *d_lines);
+          d_src, nlines, ninner, so, se, si, ns, h, d_coef, d_coef + ns, d_scratch, *d_lines,
+          d_weights);
       ctx->launches++;
       st = wrt::check_launch(ctx, "spline_prep_kernel");
       if (!st) {
@@ -156,10 +161,10 @@ namespace wrt {
 // Radon data set ([nshift][nphi][ntheta]) and the adjoint proper.
 int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
                          const double *d_cp, const double *d_den, double *d_scratch,
-                         float4 *d_lines) {
+                         float4 *d_lines, const double4 *d_dirw) {
   spline_prep_kernel<<<(ndir + 127) / 128, 128, 0, stream>>>(
       d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, 2.0 / (nshift - 1), d_cp, d_den,
-      d_scratch, d_lines);
+      d_scratch, d_lines, d_dirw);
   return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
 }
 
@@ -179,7 +184,7 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
   float4 *d_lines = nullptr;
   size_t bytes = 0;
   int st = prep_lines(ctx, d_rays, ngrid * nphi, nphi, (long long)nshift_ray * nphi, nphi, 1,
-                      nshift_ray, &d_lines, &bytes);
+                      nshift_ray, &d_lines, &bytes, nullptr);
   if (st) return st;
   const long long total = (long long)nshift * nphi * ntheta;
   const long long blocks = (total + 255) / 256;
@@ -201,7 +206,8 @@ int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, i
   float4 *d_lines = nullptr;
   size_t bytes = 0;
   const int ndir = nphi * ntheta;
-  int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, &bytes);
+  int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, &bytes,
+                      d_dirw);
   if (st) return st;
   const long long items = wrtd::adjoint_items(n);
   adjoint_kernel<<<(unsigned)((items + 255) / 256), 256, 0, ctx->stream>>>(

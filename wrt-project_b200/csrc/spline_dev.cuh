@@ -17,10 +17,13 @@ namespace wrtd {
 // Tridiagonal solve of one line (Thomas algorithm in FP64).  y(i) is element
 // i of the line, read through y + i * se.  cp / den: the line-independent
 // forward-elimination coefficients of M_{i-1} + 4 M_i + M_{i+1} = rhs_i.
+// scale: a weight the stored values and curvatures are multiplied by in FP64
+// before their rounding to FP32 (the spline of scale * y; 1 for plain lines).
 __device__ __forceinline__ void spline_line(const double *__restrict__ y, long long se, int ns,
                                             double h, const double *__restrict__ cp,
                                             const double *__restrict__ den,
-                                            double *__restrict__ M, float4 *__restrict__ o) {
+                                            double *__restrict__ M, float4 *__restrict__ o,
+                                            double scale = 1.0) {
   M[0] = 0.0;
   M[ns - 1] = 0.0;
   const double six_h2 = 6.0 / (h * h);
@@ -33,7 +36,8 @@ __device__ __forceinline__ void spline_line(const double *__restrict__ y, long l
   }
   for (int i = ns - 3; i >= 1; --i) M[i] = M[i] - cp[i] * M[i + 1];
   for (int i = 0; i + 1 < ns; ++i)
-    o[i] = make_float4((float)y[i * se], (float)y[(i + 1) * se], (float)M[i], (float)M[i + 1]);
+    o[i] = make_float4((float)(scale * y[i * se]), (float)(scale * y[(i + 1) * se]),
+                       (float)(scale * M[i]), (float)(scale * M[i + 1]));
 }
 
 // The same at a knot position q given in FP64, 0 <= q <= ns - 1 (the
@@ -66,10 +70,11 @@ __device__ __forceinline__ float spline_eval(const float4 *__restrict__ line, in
 // it reads dirw once and steps the knot position q = (s + 1)/h from voxel to
 // voxel by one FP64 add, q and its fraction in FP64 (dirw holds the
 // reference's FP64 omega; a few FP64 roundings from the direct dot product,
-// 1e-14 knots at most), the spline value and its weight in FP32, the sum over
-// directions in FP64.  |s| <= 1 is tested as 0 <= q <= ns - 1.  Threads of a
-// warp take consecutive iy: one direction's 32 lanes read neighbouring knot
-// intervals of one line.
+// 1e-14 knots at most), the spline value in FP32 (each direction's weight is
+// folded into its line's values and curvatures in FP64 when the line is
+// built), the sum over directions in FP64.  |s| <= 1 is tested as
+// 0 <= q <= ns - 1.  Threads of a warp take consecutive iy: one direction's
+// 32 lanes read neighbouring knot intervals of one line.
 constexpr int kAdjVoxels = 4;
 
 // thread items of an n^3 adjoint: (iz, ix group, iy), iy fastest
@@ -98,7 +103,6 @@ __device__ __forceinline__ void adjoint_item(const float4 *__restrict__ lines, i
   for (int d = 0; d < ndir; ++d) {
     const double2 w01 = __ldg(reinterpret_cast<const double2 *>(dirw + d));
     const double2 w23 = __ldg(reinterpret_cast<const double2 *>(dirw + d) + 1);
-    const float wf = (float)w23.y;
     const double q0 = fma(fma(x0, w01.x, fma(y, w01.y, z * w23.x)), inv_hs, inv_hs);
     const double qs = qdx * w01.x;
     const float4 *line = lines + d * line_len;
@@ -106,7 +110,7 @@ __device__ __forceinline__ void adjoint_item(const float4 *__restrict__ lines, i
     for (int v = 0; v < kAdjVoxels; ++v) {
       const double q = fma((double)v, qs, q0);
       if (q >= 0.0 && q <= qmax)
-        acc[v] += (double)__fmul_rn(wf, spline_eval_q64(line, ns, q, h2_6));
+        acc[v] += (double)spline_eval_q64(line, ns, q, h2_6);  // line holds w_d * S_d
     }
   }
   const size_t base = ((size_t)iz * n + ix0) * n + iy;
