@@ -99,7 +99,7 @@ __device__ __forceinline__ void adjoint_item(const float4 *__restrict__ lines, i
   double acc[kAdjVoxels];
 #pragma unroll
   for (int v = 0; v < kAdjVoxels; ++v) acc[v] = 0.0;
-#pragma unroll 2
+#pragma unroll 4
   for (int d = 0; d < ndir; ++d) {
     const double2 w01 = __ldg(reinterpret_cast<const double2 *>(dirw + d));
     const double2 w23 = __ldg(reinterpret_cast<const double2 *>(dirw + d) + 1);
