@@ -55,6 +55,7 @@ __global__ void __launch_bounds__(256)
   const double p = shift[is], ct = cs[2 * it], st = cs[2 * it + 1];
   const double dtau = (2.0 / (ngrid - 1)) / (2.0);  // slicing.c:88
   const double delta_z = 2.0 / (ngrid - 1);         // slicing.c:18
+  const double inv_dz = 0.5 * (ngrid - 1);
   const float hs = 2.0f / (float)(ns_ray - 1);
   const float inv_hs = 1.0f / hs;
   const float h2_6 = hs * hs / 6.0f;
@@ -75,10 +76,15 @@ __global__ void __launch_bounds__(256)
     if ((fabs(__dadd_rn(__dmul_rn(tau, tau), __dmul_rn(p, p))) > 1.0) || (fabs(z) > 1.0) ||
         (fabs(s) > 1.0))
       continue;
-    int iz = (int)__ddiv_rn(__dadd_rn(z, 1.0), delta_z);
+    // layer index of slicing.c:15-20, (int)((z + 1) / delta_z): by the
+    // reciprocal, and by the division itself where the quotient lies within
+    // 1e-9 of an integer (the reciprocal's error is ~1e-14 there)
+    const double z1 = __dadd_rn(z, 1.0), qz = z1 * inv_dz;
+    int iz = (int)qz;
+    if (fabs(qz - rint(qz)) < 1e-9) iz = (int)__ddiv_rn(z1, delta_z);
     if (iz == ngrid - 1) iz -= 1;
     const double z0 = __dadd_rn(-1.0, __dmul_rn(delta_z, (double)iz));
-    const float f = (float)((z - z0) / delta_z);
+    const float f = (float)((z - z0) * inv_dz);
     const float q = (float)(s + 1.0) * inv_hs;
     const float4 *l0 = lines + ((size_t)iz * nphi + ip) * line_len;
     const float v0 = wrtd::spline_eval(l0, ns_ray, q, h2_6);
