@@ -190,6 +190,7 @@ int wrt_ctx_create(int device, size_t budget, wrt_ctx **out) {
     delete ctx;
     return WRT_ERR_CUDA;
   }
+  noalloc_forget_device(device);
   *out = ctx;
   return WRT_OK;
 }
@@ -876,12 +877,7 @@ int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
   st = sphere_grid(ctx, nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), shift.data());
   const int ndir = nphi * ntheta;
   std::vector<double4> dirw(ndir);
-  const double dphi = 2 * M_PI / nphi;  // backprojection/C/src/integral.c:11
-  for (int ip = 0; ip < nphi; ++ip)
-    for (int it = 0; it < ntheta; ++it)
-      dirw[ip * ntheta + it] = make_double4(sin(theta[it]) * cos(phi[ip]),
-                                            sin(theta[it]) * sin(phi[ip]), cos(theta[it]),
-                                            dphi * w[it]);
+  adjoint_directions(nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), dirw.data());
   DevBuf dradon(ctx), ddirw(ctx), dout(ctx);
   const size_t nin = (size_t)nshift * ndir, nout = (size_t)ngrid * ngrid * ngrid;
   if (!st) st = dradon.alloc(sizeof(double) * nin);

@@ -151,23 +151,31 @@ __global__ void batch_spline_kernel(const char *t) {
   for (int r = 0; r < na; ++r) {
     const int ns = J[r].nshift, nd = J[r].ndir;
     for (long long L = tid; L < nd; L += nth)
-      wrtd::spline_line(J[r].radon + L, nd, ns, 2.0 / (ns - 1), J[r].cp, J[r].den,
-                        J[r].scratch + (size_t)L * ns, J[r].lines + (size_t)L * (ns - 1),
-                        J[r].dirw[L].w);  // the direction's quadrature weight
+      wrtd::spline_line_centred(J[r].radon + L, nd, ns, 2.0 / (ns - 1), J[r].cp, J[r].den,
+                                J[r].scratch + (size_t)L * ns, J[r].lines + (size_t)L * (ns - 1),
+                                J[r].dirw[L].w);  // the direction's quadrature weight
   }
 }
 
-// Backprojection of every voxel of every adjoint request.
-__global__ void __launch_bounds__(256) batch_adjoint_kernel(const char *t) {
+// Backprojection of every voxel of every adjoint request: the voxel-block
+// warps of all requests, taken in turn by the grid's warps.
+__global__ void __launch_bounds__(256, 2) batch_adjoint_kernel(const char *t) {
   const int na = hdr(t)->nadj;
   const AdjReq *J = adj_tab(t);
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nth = (long long)gridDim.x * blockDim.x;
+  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+  const long long nw = (long long)gridDim.x * blockDim.x / 32;
+  const int lane = threadIdx.x & 31;
+  long long first = 0;  // global index of request r's first warp
   for (int r = 0; r < na; ++r) {
     const int n = J[r].n;
-    const long long items = wrtd::adjoint_items(n);
-    for (long long t2 = tid; t2 < items; t2 += nth)
-      wrtd::adjoint_item(J[r].lines, J[r].ndir, J[r].nshift, J[r].dirw, n, t2, J[r].out);
+    const long long warps = wrtd::adjoint_warps(n);
+    // warps continue from one request to the next so that small requests do
+    // not leave most of the grid idle
+    long long w = gw - first % nw;
+    if (w < 0) w += nw;
+    for (; w < warps; w += nw)
+      wrtd::adjoint_block(J[r].lines, J[r].ndir, J[r].nshift, J[r].dirw, n, w, lane, J[r].out);
+    first += warps;
   }
 }
 

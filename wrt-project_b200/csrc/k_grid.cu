@@ -22,7 +22,7 @@
 
 namespace {
 
-__device__ double series_cos(double a) {
+__host__ __device__ double series_cos(double a) {
   double a2 = a * a, term = 1.0, sum = 1.0;
   for (int k = 1; k <= 30; ++k) {
     double den = (double)((2 * k - 1) * (2 * k));
@@ -32,7 +32,7 @@ __device__ double series_cos(double a) {
   return sum;
 }
 
-__device__ void legendre_pair(int n, double x, double *pn, double *pnm1) {
+__host__ __device__ void legendre_pair(int n, double x, double *pn, double *pnm1) {
   double p0 = 1.0, p1 = x;
   if (n == 0) {
     *pn = 1.0;
@@ -52,16 +52,16 @@ __device__ void legendre_pair(int n, double x, double *pn, double *pnm1) {
   *pnm1 = p0;
 }
 
-__device__ double legendre_deriv(int n, double r, double pn, double pnm1) {
+__host__ __device__ double legendre_deriv(int n, double r, double pn, double pnm1) {
   double num = (double)n * (r * pn - pnm1);
   double den = r * r - 1.0;
   return num / den;
 }
 
-// One thread per positive root (k = 1..n/2) plus one for the middle node.
-__global__ void gl_nodes_kernel(int n, double *x, double *w) {
+// Root k (1 <= k <= n/2) and its weight; k = n/2 + 1 for odd n: the middle
+// node.  Writes the mirrored pair into x / w (ascending order).
+__host__ __device__ void gl_root(int n, int k, double *x, double *w) {
   const int m = n / 2;
-  int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (k <= m) {
     double ang = (WRT_PI * ((double)k - 0.25)) / ((double)n + 0.5);
     double r = series_cos(ang);
@@ -87,6 +87,11 @@ __global__ void gl_nodes_kernel(int n, double *x, double *w) {
     x[m] = 0.0;
     w[m] = 2.0 / ((1.0 * dp) * dp);
   }
+}
+
+// One thread per positive root (k = 1..n/2) plus one for the middle node.
+__global__ void gl_nodes_kernel(int n, double *x, double *w) {
+  gl_root(n, blockIdx.x * blockDim.x + threadIdx.x + 1, x, w);
 }
 
 }  // namespace
@@ -133,12 +138,26 @@ int sphere_grid(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *phi, dou
   return WRT_OK;
 }
 
-// Gauss-Legendre nodes into caller-provided device memory, on a given stream
-// (used by the allocation-free adjoint entry point).
-int launch_gl_nodes(cudaStream_t stream, int n, double *d_x, double *d_w) {
-  const int threads = 128, blocks = (n / 2 + 1 + threads - 1) / threads;
-  gl_nodes_kernel<<<blocks, threads, 0, stream>>>(n, d_x, d_w);
-  return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
+// The same rule on the host (the host compiler emits no fused multiply-add
+// here, so the nodes are those of gl_nodes_kernel bit for bit); used where a
+// caller's path may not allocate device memory.
+void gauss_legendre_host(int n, double *x, double *w) {
+  for (int k = 1; k <= n / 2 + 1; ++k) gl_root(n, k, x, w);
+}
+
+// Backprojection direction table: dirw[ip*ntheta + it] = (omega / h,
+// dphi * w_theta) with omega = (sin t cos p, sin t sin p, cos t) in the
+// reference's expression order (backprojection/C/src/integral.c:11-18) and
+// h = 2/(nshift-1), so that <x, omega>/h + 1/h is a voxel's knot position.
+void adjoint_directions(int nphi, int ntheta, int nshift, const double *phi, const double *theta,
+                        const double *theta_w, double4 *dirw) {
+  const double dphi = 2 * M_PI / nphi;
+  const double inv_h = 0.5 * (double)(nshift - 1);
+  for (int ip = 0; ip < nphi; ++ip)
+    for (int it = 0; it < ntheta; ++it)
+      dirw[(size_t)ip * ntheta + it] =
+          make_double4(sin(theta[it]) * cos(phi[ip]) * inv_h, sin(theta[it]) * sin(phi[ip]) * inv_h,
+                       cos(theta[it]) * inv_h, dphi * theta_w[it]);
 }
 
 // radon_grid/src/integral.c:10-36: normal = omega(phi, theta),

@@ -1,36 +1,40 @@
 // k_noalloc.cu -- the adjoint (backprojection) without any device allocation.
 //
 // wrt_radon3d_adjoint allocates its working memory (spline tables, direction
-// table, Gauss-Legendre nodes) with cudaMalloc on every call.  Some callers
-// cannot allow that: programs that hand all device memory to their own
-// allocator or reserve it up front (a cudaMalloc then fails, or fragments the
-// reservation), and latency-critical pipelines that forbid allocation after
-// start-up because cudaMalloc/cudaFree synchronise the whole device and stall
-// every other stream.  wrt_radon3d_adjoint_static serves them: the caller
-// passes device input and output buffers, and all working memory lives in one
-// file-scope __device__ array of fixed size (kScratchBytes below), which every
-// GPU that loads this library holds until the process exits.
+// table) with cudaMalloc on every call.  Some callers cannot allow that:
+// programs that hand all device memory to their own allocator or reserve it
+// up front (a cudaMalloc then fails, or fragments the reservation), and
+// latency-critical pipelines that forbid allocation after start-up because
+// cudaMalloc/cudaFree synchronise the whole device and stall every other
+// stream.  wrt_radon3d_adjoint_static serves them: the caller passes device
+// input and output buffers, and all working memory lives in one file-scope
+// __device__ array of fixed size (kScratchBytes below), which every GPU that
+// loads this library holds until the process exits.
 //
 // Limits (checked, WRT_ERR_INVALID_ARGUMENT with a message otherwise):
 //   nphi * ntheta <= 16384 directions, ntheta <= 1024, 3 <= nshift <= 2048,
 //   nphi * ntheta * nshift <= 262144 spline samples.
-// The scratch array is shared by every call on a device and keeps the last
-// call's contents; every call writes all of it that it reads before reading,
-// so nothing has to start at zero.  Calls whose GPU work overlaps (different
-// streams, or different host threads) race on the array: order them.
+// The small tables (direction weights, spline elimination coefficients) are
+// computed on the host by the same code as wrt_radon3d_adjoint's, Gauss-
+// Legendre nodes included, and copied into the array from host memory, so the
+// two entry points give bitwise the same volume.  The array is shared by every
+// call on a device and keeps the last call's contents; every call writes all
+// of it that it reads before reading, so nothing has to start at zero.  Calls
+// whose GPU work overlaps (different streams, or different host threads) race
+// on the array: order them.
 #include <math.h>
 
 #include <mutex>
+#include <vector>
 
 #include "wrt_internal.cuh"
 
 namespace wrt {
-int launch_gl_nodes(cudaStream_t stream, int n, double *d_x, double *d_w);
-int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
-                         const double *d_cp, const double *d_den, double *d_scratch,
-                         float4 *d_lines, const double4 *d_dirw);
-int launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int ntheta, int nshift,
-                   const double4 *d_dirw, int n, double *d_out);
+cudaError_t launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
+                                 const double *d_cp, const double *d_den, double *d_scratch,
+                                 float4 *d_lines, const double4 *d_dirw);
+cudaError_t launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int nshift,
+                           const double4 *d_dirw, int n, double *d_out);
 }  // namespace wrt
 
 namespace {
@@ -39,47 +43,17 @@ constexpr int kMaxDirs = 16384, kMaxTheta = 1024, kMaxShift = 2048;
 constexpr long long kMaxEntries = 262144;  // nphi * ntheta * nshift
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-constexpr size_t kOffX = 0;
-constexpr size_t kOffW = align256(kOffX + sizeof(double) * kMaxTheta);
-constexpr size_t kOffCp = align256(kOffW + sizeof(double) * kMaxTheta);
+constexpr size_t kOffCp = 0;
 constexpr size_t kOffDen = align256(kOffCp + sizeof(double) * kMaxShift);
 constexpr size_t kOffDirw = align256(kOffDen + sizeof(double) * kMaxShift);
 constexpr size_t kOffM = align256(kOffDirw + sizeof(double4) * kMaxDirs);
 constexpr size_t kOffLines = align256(kOffM + sizeof(double) * kMaxEntries);
 constexpr size_t kScratchBytes = align256(kOffLines + sizeof(float4) * kMaxEntries);
 
-// The working memory (about 6.6 MB).  In host code this name is a host-side
+// The working memory (about 6.8 MB).  In host code this name is a host-side
 // stand-in, not a device address: host code must use the address returned by
 // cudaGetSymbolAddress (scratch_base below).
 static __device__ __align__(256) unsigned char g_adjoint_scratch[kScratchBytes];
-
-// Line-independent elimination coefficients of the uniform-knot natural
-// spline system M_{i-1} + 4 M_i + M_{i+1} = rhs_i (same values as the host
-// computation in k_spline.cu).
-__global__ void spline_coef_kernel(int ns, double *cp, double *den) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  cp[0] = 0.0;
-  den[0] = 1.0;
-  cp[ns - 1] = 0.0;
-  den[ns - 1] = 1.0;
-  for (int i = 1; i + 1 < ns; ++i) {
-    den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);
-    cp[i] = 1.0 / den[i];
-  }
-}
-
-// dirw[ip*ntheta + it] = (sin t cos p, sin t sin p, cos t, dphi * w_t),
-// t = acos(GL node), p = 2 pi ip / nphi
-// (backprojection/C/src/init.c:222-245 and integral.c:11-18).
-__global__ void direction_weights_kernel(int nphi, int ntheta, const double *x, const double *w,
-                                         double4 *dirw) {
-  const int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d >= nphi * ntheta) return;
-  const int ip = d / ntheta, it = d - ip * ntheta;
-  const double dphi = (2 * WRT_PI) / nphi;
-  const double p = dphi * ip, t = acos(x[it]);
-  dirw[d] = make_double4(sin(t) * cos(p), sin(t) * sin(p), cos(t), dphi * w[it]);
-}
 
 std::mutex g_setup_mutex;
 void *g_scratch_base[64] = {nullptr};
@@ -102,6 +76,15 @@ int scratch_base(wrt_ctx *ctx, unsigned char **base) {
 
 }  // namespace
 
+namespace wrt {
+// Forgets the cached address of the scratch array on a device.  Called when a
+// context is created: a device reset before it would have moved the array.
+void noalloc_forget_device(int device) {
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (device >= 0 && device < 64) g_scratch_base[device] = nullptr;
+}
+}  // namespace wrt
+
 extern "C" int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, int nphi,
                                           int ntheta, int nshift, int ngrid, double *d_out) {
   if (!ctx) return WRT_ERR_INVALID_ARGUMENT;
@@ -119,23 +102,46 @@ extern "C" int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, i
   unsigned char *base = nullptr;
   int st = scratch_base(ctx, &base);
   if (st) return st;
-  double *x = reinterpret_cast<double *>(base + kOffX);
-  double *w = reinterpret_cast<double *>(base + kOffW);
   double *cp = reinterpret_cast<double *>(base + kOffCp);
   double *den = reinterpret_cast<double *>(base + kOffDen);
   double4 *dirw = reinterpret_cast<double4 *>(base + kOffDirw);
   double *M = reinterpret_cast<double *>(base + kOffM);
   float4 *lines = reinterpret_cast<float4 *>(base + kOffLines);
-  cudaStream_t s = ctx->stream;
-  st = wrt::launch_gl_nodes(s, ntheta, x, w);
-  if (!st) {
-    spline_coef_kernel<<<1, 1, 0, s>>>(nshift, cp, den);
-    direction_weights_kernel<<<(int)((ndir + 127) / 128), 128, 0, s>>>(nphi, ntheta, x, w, dirw);
-    st = cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
+  // host tables: the sphere grid (radon_grid/src/init.c:165-189, GL nodes by
+  // the GPU generator's own code), the direction weights and the natural
+  // spline elimination coefficients, exactly as wrt_radon3d_adjoint builds them
+  std::vector<double> x(ntheta), w(ntheta), theta(ntheta), phi(nphi);
+  wrt::gauss_legendre_host(ntheta, x.data(), w.data());
+  for (int i = 0; i < ntheta; ++i) theta[i] = acos(x[i]);
+  const double dphi = (2 * M_PI) / nphi;
+  for (int i = 0; i < nphi; ++i) phi[i] = dphi * i;
+  std::vector<double4> h_dirw((size_t)ndir);
+  wrt::adjoint_directions(nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), h_dirw.data());
+  std::vector<double> coef(2 * (size_t)nshift);
+  double *h_cp = coef.data(), *h_den = coef.data() + nshift;
+  for (int i = 0; i < nshift; ++i) {
+    h_cp[i] = 0.0;
+    h_den[i] = 1.0;
   }
-  if (!st) st = wrt::launch_adjoint_lines(s, d_radon, (int)ndir, nshift, cp, den, M, lines, dirw);
-  if (!st) st = wrt::launch_adjoint(s, lines, (int)ndir, ntheta, nshift, dirw, ngrid, d_out);
-  ctx->launches += 5;
-  if (st) return wrt::fail(ctx, WRT_ERR_CUDA, "radon3d_adjoint_static: launch failed");
+  for (int i = 1; i + 1 < nshift; ++i) {
+    h_den[i] = 4.0 - (i > 1 ? h_cp[i - 1] : 0.0);
+    h_cp[i] = 1.0 / h_den[i];
+  }
+  // copies from pageable host memory return once the data is staged, so the
+  // vectors may go out of scope before the copies land
+  cudaStream_t s = ctx->stream;
+  e = cudaMemcpyAsync(dirw, h_dirw.data(), sizeof(double4) * (size_t)ndir,
+                      cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(cp, h_cp, sizeof(double) * nshift, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(den, h_den, sizeof(double) * nshift, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "radon3d_adjoint_static: table upload");
+  e = wrt::launch_adjoint_lines(s, d_radon, (int)ndir, nshift, cp, den, M, lines, dirw);
+  if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "radon3d_adjoint_static: spline_prep_kernel");
+  ctx->launches++;
+  e = wrt::launch_adjoint(s, lines, (int)ndir, nshift, dirw, ngrid, d_out);
+  if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "radon3d_adjoint_static: adjoint_kernel");
+  ctx->launches++;
   return WRT_OK;
 }

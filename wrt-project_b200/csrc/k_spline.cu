@@ -7,11 +7,9 @@
 // A line's spline depends only on that line, so here it is built once:
 // spline_prep_kernel solves the natural-spline tridiagonal system of every
 // line (uniform knots s_i = -1 + i h, h = 2/(ns-1), end conditions M_0 =
-// M_{ns-1} = 0) in FP64 and stores, per knot interval, the float4
-// (y_i, y_{i+1}, M_i, M_{i+1}).  An evaluation is then one 16-byte load and
-//   S(s) = a y_i + b y_{i+1} + ((a^3 - a) M_i + (b^3 - b) M_{i+1}) h^2 / 6,
-//   b = (s - s_i)/h, a = 1 - b,
-// the same piecewise cubic as the reference's spline.
+// M_{ns-1} = 0) in FP64 and stores one float4 per knot interval (the record
+// forms are described in spline_dev.cuh); an evaluation is one 16-byte load
+// and the same piecewise cubic as the reference's spline.
 #include <vector>
 
 #include "spline_dev.cuh"
@@ -33,10 +31,15 @@ __global__ void spline_prep_kernel(const double *__restrict__ src, int nlines, i
   const int L = blockIdx.x * blockDim.x + threadIdx.x;
   if (L >= nlines) return;
   const int outer = L / ninner, inner = L % ninner;
-  // adjoint lines carry their direction's quadrature weight dphi * w_theta
-  const double scale = weights ? weights[L].w : 1.0;
-  wrtd::spline_line(src + outer * so + inner * si, se, ns, h, cp, den, scratch + (size_t)L * ns,
-                    out + (size_t)L * (ns - 1), scale);
+  // adjoint lines (weights given): centred power form scaled by the
+  // direction's quadrature weight dphi * w_theta; reduction lines: values and
+  // curvatures
+  if (weights)
+    wrtd::spline_line_centred(src + outer * so + inner * si, se, ns, h, cp, den,
+                              scratch + (size_t)L * ns, out + (size_t)L * (ns - 1), weights[L].w);
+  else
+    wrtd::spline_line(src + outer * so + inner * si, se, ns, h, cp, den, scratch + (size_t)L * ns,
+                      out + (size_t)L * (ns - 1));
 }
 
 // Reduction: one thread per Radon sample (is, iphi, itheta), order of
@@ -98,16 +101,18 @@ __global__ void __launch_bounds__(256)
   out[k] = acc * dtau;
 }
 
-// Adjoint: one thread per wrtd::kAdjVoxels voxels along x, output order
-// [iz][ix][iy]; loop over all directions.  dirw[d] = (sin t cos p,
-// sin t sin p, cos t, dphi * w_t).
-__global__ void __launch_bounds__(256)
+// Adjoint: one warp per voxel block of wrtd::adjoint_block (8 x 4 columns of
+// V voxels), output order [iz][ix][iy]; every lane loops over all directions.
+// dirw[d] = (omega / h, dphi * w_theta).
+__global__ void __launch_bounds__(256, 3)
     adjoint_kernel(const float4 *__restrict__ lines /* [d][ns-1] */, int ndir, int ns,
                    const double4 *__restrict__ dirw, int n, double *__restrict__ out) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= wrtd::adjoint_items(n)) return;
-  wrtd::adjoint_item(lines, ndir, ns, dirw, n, t, out);
+  const long long w = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (w >= wrtd::adjoint_warps(n)) return;
+  wrtd::adjoint_block(lines, ndir, ns, dirw, n, w, threadIdx.x & 31, out);
 }
+
+unsigned adjoint_blocks(int n) { return (unsigned)((wrtd::adjoint_warps(n) + 7) / 8); }
 
 int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long long so,
                long long se, long long si, int ns, float4 **d_lines, size_t *bytes,
@@ -165,22 +170,19 @@ namespace wrt {
 // Launchers over caller-provided device memory (used by the allocation-free
 // adjoint entry point): spline preparation of the nphi*ntheta lines of a
 // Radon data set ([nshift][nphi][ntheta]) and the adjoint proper.
-int launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
-                         const double *d_cp, const double *d_den, double *d_scratch,
-                         float4 *d_lines, const double4 *d_dirw) {
+cudaError_t launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
+                                 const double *d_cp, const double *d_den, double *d_scratch,
+                                 float4 *d_lines, const double4 *d_dirw) {
   spline_prep_kernel<<<(ndir + 127) / 128, 128, 0, stream>>>(
       d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, 2.0 / (nshift - 1), d_cp, d_den,
       d_scratch, d_lines, d_dirw);
-  return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
+  return cudaGetLastError();
 }
 
-int launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int ntheta, int nshift,
-                   const double4 *d_dirw, int n, double *d_out) {
-  (void)ntheta;
-  const long long items = wrtd::adjoint_items(n);
-  adjoint_kernel<<<(unsigned)((items + 255) / 256), 256, 0, stream>>>(d_lines, ndir, nshift,
-                                                                        d_dirw, n, d_out);
-  return cudaGetLastError() == cudaSuccess ? WRT_OK : WRT_ERR_CUDA;
+cudaError_t launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int nshift,
+                           const double4 *d_dirw, int n, double *d_out) {
+  adjoint_kernel<<<adjoint_blocks(n), 256, 0, stream>>>(d_lines, ndir, nshift, d_dirw, n, d_out);
+  return cudaGetLastError();
 }
 
 int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_ray, int nphi,
@@ -215,9 +217,8 @@ int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, i
   int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, &bytes,
                       d_dirw);
   if (st) return st;
-  const long long items = wrtd::adjoint_items(n);
-  adjoint_kernel<<<(unsigned)((items + 255) / 256), 256, 0, ctx->stream>>>(
-      d_lines, ndir, nshift, d_dirw, n, d_out);
+  adjoint_kernel<<<adjoint_blocks(n), 256, 0, ctx->stream>>>(d_lines, ndir, nshift, d_dirw, n,
+                                                              d_out);
   ctx->launches++;
   st = check_launch(ctx, "adjoint_kernel");
   if (!st) {

@@ -150,12 +150,7 @@ int make_grid(wrt_server *s, GridTables &g) {
   // backprojection weights (backprojection/C/src/integral.c:11-18) and the
   // natural-spline elimination coefficients
   std::vector<double4> dirw(ndir);
-  const double dphi = 2 * M_PI / nphi;
-  for (int ip = 0; ip < nphi; ++ip)
-    for (int it = 0; it < ntheta; ++it)
-      dirw[ip * ntheta + it] = make_double4(sin(theta[it]) * cos(phi[ip]),
-                                            sin(theta[it]) * sin(phi[ip]), cos(theta[it]),
-                                            dphi * w[it]);
+  wrt::adjoint_directions(nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), dirw.data());
   std::vector<double> cp(nshift, 0.0), den(nshift, 1.0);
   for (int i = 1; i + 1 < nshift; ++i) {
     den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);

@@ -75,6 +75,12 @@ void plane_directions(int nphi, const double *phi, int ntheta, const double *the
 int sphere_grid(wrt_ctx *ctx, int nphi, int ntheta, int nshift, double *phi,
                 double *theta, double *theta_w, double *shift);
 int gauss_legendre_device(wrt_ctx *ctx, int n, double *x_host, double *w_host);
+// The same nodes computed on the host (bit-identical to the GPU's).
+void gauss_legendre_host(int n, double *x, double *w);
+// Backprojection direction table [nphi*ntheta]: (omega / h, dphi * w_theta),
+// h = 2/(nshift-1).
+void adjoint_directions(int nphi, int ntheta, int nshift, const double *phi, const double *theta,
+                        const double *theta_w, double4 *dirw);
 
 // Volume preparation kernels (k_volume.cu).
 // d_stats[0]: largest |x|^2 of a non-zero node, d_stats[1]: max |v| (float bits)
@@ -185,7 +191,7 @@ struct FwdAux {                    // per forward request, beside its StagedReq
 };
 struct AdjReq {                    // one backprojection
   const double *radon;             // [is][iphi][itheta]
-  const double4 *dirw;             // [ndir]: omega, dphi * w_theta (FP64)
+  const double4 *dirw;             // [ndir]: omega / h, dphi * w_theta (FP64)
   const double *cp, *den;          // spline elimination coefficients [nshift]
   double *scratch;                 // [ndir][nshift]
   float4 *lines;                   // [ndir][nshift - 1]
@@ -260,6 +266,10 @@ struct RayJob {
 };
 int ray_forward(wrt_ctx *ctx, const RayJob &job);
 
+// Allocation-free backprojection (k_noalloc.cu): drops the cached device
+// address of its working array on a device (a new context may follow a reset).
+void noalloc_forget_device(int device);
+
 // Shared-memory bandwidth microbenchmark (k_probe.cu).
 int smem_bandwidth(wrt_ctx *ctx, double *bytes_per_s);
 
@@ -269,7 +279,7 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
                       const double *d_cs /* [ntheta][2]: cos, sin theta */, int ntheta,
                       double *d_out);
 int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
-                    const double4 *d_dirw /* [nphi*ntheta]: omega, dphi*w */, int n,
+                    const double4 *d_dirw /* [nphi*ntheta]: omega/h, dphi*w */, int n,
                     double *d_out);
 
 }  // namespace wrt
