@@ -12,7 +12,9 @@
  * host buffers out, same array orders as the programs' text files), plus
  * device-resident objects for serving.  Every call returns a wrt_status; no
  * call exits the process.  There is no CPU fallback: without a usable CUDA
- * device the calls fail with WRT_ERR_NO_DEVICE.
+ * device the calls fail with WRT_ERR_NO_DEVICE.  The drop-in entry points
+ * keep their device buffers in the context between calls: a warm call of the
+ * same or smaller sizes allocates no device memory.
  *
  * Array orders (flat, row-major):
  *   volume  v[ix][iy][iz]          (radon_grid/src/init.c:120-124)
@@ -139,7 +141,9 @@ int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
  * <= 16384, ntheta <= 1024, 3 <= nshift <= 2048, nphi*ntheta*nshift <=
  * 262144; larger sizes return WRT_ERR_INVALID_ARGUMENT with a message.  The
  * first call on a device looks up the array's device address (make that first
- * call before any stream capture).  Asynchronous on the context's stream.
+ * call before any stream capture); creating a context forgets it again, so
+ * after a device reset create new contexts before calling.  Asynchronous on
+ * the context's stream.
  * Every call shares the array: calls whose GPU work overlaps (other streams,
  * other contexts on the same device) race and must be ordered by the caller. */
 int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta,
@@ -182,6 +186,32 @@ int wrt_grid_destroy(wrt_grid *grid);
  * the context's stream. */
 int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *grid,
                              const wrt_plane_opts *opts, double *dev_out);
+
+/* Ray integrals of a resident FP32 volume into a device buffer of
+ * nslices*nshift*nphi doubles, order [iz][is][iphi] as wrt_ray_grid.  frame:
+ * NULL (the reference's z-slices) or a row-major 3x3 rotation in host memory.
+ * Asynchronous on the context's stream; small tables and the volume's layer
+ * pairs live in the context (no allocation once warm).  Device-resident form of
+ * ray_grid/src/ray_grid.c:225-262 with ray_transform (integral.c:11-50). */
+int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *vol, const double *frame,
+                           int nslices, int nshift, int nphi, double *dev_out);
+
+/* Reduction of device ray data dev_rays[iz][is_ray][iphi] (ngrid z-slices,
+ * nshift_ray offsets, grid->nphi angles) to Radon data on a resident sphere
+ * grid, dev_out[is][iphi][itheta] (nshift * nphi * ntheta doubles of the
+ * grid).  Asynchronous; spline working memory lives in the context.
+ * Device-resident form of radon_reduction/reduction.c:195-235 with
+ * radon_reduction and ray_interpolate (slicing.c:5-119). */
+int wrt_radon_reduction_device(wrt_ctx *ctx, const double *dev_rays, int ngrid, int nshift_ray,
+                               const wrt_grid *grid, double *dev_out);
+
+/* Backprojection of device Radon data dev_radon[is][iphi][itheta] on a
+ * resident sphere grid into dev_out, ngrid^3 doubles [iz][ix][iy].
+ * Asynchronous; spline working memory lives in the context.  Device-resident
+ * form of backprojection/C/src/radon3d_ajoint.c:221-260 with radon3d_adjoint
+ * (integral.c:6-24). */
+int wrt_radon3d_adjoint_device(wrt_ctx *ctx, const double *dev_radon, const wrt_grid *grid,
+                               int ngrid, double *dev_out);
 
 /* One request of a batch: the plane integrals of a resident volume on a
  * resident sphere grid (trilinear sampler, lattice [-L, L)^2 with step 1/n,

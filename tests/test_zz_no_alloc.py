@@ -42,9 +42,9 @@ def test_static_adjoint_matches_allocating_adjoint_on_two_calls():
     with wrt.Context(0) as ctx:
         din = wrt.DeviceBuffer(ctx, nshift * nphi * ntheta * 8)
         dout = wrt.DeviceBuffer(ctx, n ** 3 * 8)
-        held = ctx.bytes_in_use
         for call in range(2):
             radon = rng.standard_normal((nshift, nphi, ntheta))
+            held = ctx.bytes_in_use
             got = _run(ctx, radon, n, din, dout)
             assert ctx.bytes_in_use == held  # the call acquired no device memory
             ref = ctx.radon3d_adjoint(radon, n)

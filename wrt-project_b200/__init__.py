@@ -130,6 +130,10 @@ def lib() -> C.CDLL:
         L.wrt_grid_create.argtypes = [_vp, _i, _i, _i, C.POINTER(_vp)]
         L.wrt_grid_destroy.argtypes = [_vp]
         L.wrt_radon_forward_device.argtypes = [_vp, _vp, _vp, C.POINTER(PlaneOpts), _vp]
+        L.wrt_ray_forward_device.argtypes = [_vp, _vp, _vp, _i, _i, _i, _vp]
+        L.wrt_radon_reduction_device.argtypes = [_vp, _vp, _i, _i, _vp, _vp]
+        L.wrt_radon3d_adjoint_device.argtypes = [_vp, _vp, _vp, _i, _vp]
+        L.wrt_radon3d_adjoint_static.argtypes = [_vp, _vp, _i, _i, _i, _i, _vp]
         L.wrt_ctx_timer_start.argtypes = [_vp]
         L.wrt_ctx_timer_stop.argtypes = [_vp, C.POINTER(C.c_float)]
         L.wrt_ctx_flush_l2.argtypes = [_vp]
@@ -449,6 +453,38 @@ def radon_forward_device(ctx: Context, vol: Volume, grid: Grid, dev_out: int, sa
     o = plane_opts(sampler, half_extent, kernel)
     ctx.check(lib().wrt_radon_forward_device(ctx.handle, vol.handle, grid.handle, C.byref(o),
                                              _vp(dev_out)), "radon_forward_device")
+
+
+def ray_forward_device(ctx: Context, vol: Volume, nslices: int, nshift: int, nphi: int,
+                       dev_out: int, frame=None):
+    """Ray integrals of a resident volume into device memory at ``dev_out``
+    ([iz][is][iphi] doubles); asynchronous on the context's stream."""
+    f = None if frame is None else _f64(frame).reshape(9)
+    fp = None if f is None else f.ctypes.data_as(_vp)
+    ctx.check(lib().wrt_ray_forward_device(ctx.handle, vol.handle, fp, int(nslices), int(nshift),
+                                           int(nphi), _vp(dev_out)), "ray_forward_device")
+
+
+def radon_reduction_device(ctx: Context, dev_rays: int, ngrid: int, nshift_ray: int, grid: Grid,
+                           dev_out: int):
+    """Radon data on ``grid`` from device ray data [iz][is_ray][grid.nphi]."""
+    ctx.check(lib().wrt_radon_reduction_device(ctx.handle, _vp(dev_rays), int(ngrid),
+                                               int(nshift_ray), grid.handle, _vp(dev_out)),
+              "radon_reduction_device")
+
+
+def radon3d_adjoint_device(ctx: Context, dev_radon: int, grid: Grid, ngrid: int, dev_out: int):
+    """Backprojection of device Radon data on ``grid`` to ngrid^3 voxels."""
+    ctx.check(lib().wrt_radon3d_adjoint_device(ctx.handle, _vp(dev_radon), grid.handle,
+                                               int(ngrid), _vp(dev_out)), "radon3d_adjoint_device")
+
+
+def radon3d_adjoint_static(ctx: Context, dev_radon: int, nphi: int, ntheta: int, nshift: int,
+                           ngrid: int, dev_out: int):
+    """The backprojection with no device allocation (fixed working memory)."""
+    ctx.check(lib().wrt_radon3d_adjoint_static(ctx.handle, _vp(dev_radon), int(nphi), int(ntheta),
+                                               int(nshift), int(ngrid), _vp(dev_out)),
+              "radon3d_adjoint_static")
 
 
 def plane_kernel_configs():

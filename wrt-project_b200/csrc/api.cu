@@ -40,6 +40,8 @@ struct wrt_grid {
   double *d_shift = nullptr;  // [nshift]
   float *d_dir32 = nullptr;   // [nphi*ntheta][8]
   float *d_shift32 = nullptr; // [nshift]
+  double *d_cs = nullptr;     // [ntheta][2]: cos, sin theta (reduction, slicing.c:104-105)
+  double4 *d_dirw = nullptr;  // [nphi*ntheta]: omega / h, dphi * w_theta (backprojection)
   size_t bytes = 0;
 };
 
@@ -84,6 +86,26 @@ void ctx_free(wrt_ctx *ctx, void *p, size_t bytes) {
 int check_launch(wrt_ctx *ctx, const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+  return WRT_OK;
+}
+
+int ws_get(wrt_ctx *ctx, int role, size_t bytes, void **p) {
+  if (role < 0 || role >= WS_ROLES) return fail(ctx, WRT_ERR_INTERNAL, "workspace role %d", role);
+  if (bytes <= ctx->ws_bytes[role] && ctx->ws[role]) {
+    *p = ctx->ws[role];
+    return WRT_OK;
+  }
+  if (ctx->ws[role]) {  // work queued on the stream may still read the old buffer
+    cudaStreamSynchronize(ctx->stream);
+    ctx_free(ctx, ctx->ws[role], ctx->ws_bytes[role]);
+    ctx->ws[role] = nullptr;
+    ctx->ws_bytes[role] = 0;
+  }
+  const size_t want = (bytes + (1 << 16) - 1) & ~(size_t)((1 << 16) - 1);
+  int st = ctx_alloc(ctx, &ctx->ws[role], want);
+  if (st) return st;
+  ctx->ws_bytes[role] = want;
+  *p = ctx->ws[role];
   return WRT_OK;
 }
 
@@ -211,6 +233,9 @@ int wrt_ctx_destroy(wrt_ctx *ctx) {
     ctx->batch_slot = nullptr;
   }
   staged_release(ctx);
+  if (ctx->dropin_vol) wrt_volume_destroy(ctx->dropin_vol);
+  if (ctx->dropin_grid) wrt_grid_destroy(ctx->dropin_grid);
+  for (int r = 0; r < WS_ROLES; ++r) ctx_free(ctx, ctx->ws[r], ctx->ws_bytes[r]);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WRT_OK;
@@ -419,16 +444,20 @@ int wrt_volume_upload(wrt_volume *v, const double *f64, const float *f32) {
   if (st) return st;
   const size_t count = (size_t)v->n * v->n * v->n;
   const bool bf16 = v->storage == WRT_STORAGE_BF16;
-  DevBuf stage(ctx), vol32(ctx);
-  st = stage.alloc(count * (f64 ? sizeof(double) : sizeof(float)));
-  if (!st && bf16) st = vol32.alloc(count * sizeof(float));
-  float *dst = bf16 ? vol32.as<float>() : v->d_vol;
-  if (!st) st = h2d(ctx, stage.p, f64 ? (const void *)f64 : (const void *)f32, stage.bytes, "volume upload");
+  // staging (and the FP32 copy a BF16 volume is rounded from) in the context's
+  // workspace; the upload waits for the statistics, so the buffers are free
+  // again when it returns
+  const size_t in_bytes = count * (f64 ? sizeof(double) : sizeof(float));
+  void *stage = nullptr, *vol32 = nullptr;
+  st = ws_get(ctx, WS_STAGE, in_bytes, &stage);
+  if (!st && bf16) st = ws_get(ctx, WS_IN, count * sizeof(float), &vol32);
+  float *dst = bf16 ? static_cast<float *>(vol32) : v->d_vol;
+  if (!st) st = h2d(ctx, stage, f64 ? (const void *)f64 : (const void *)f32, in_bytes, "volume upload");
   if (!st)
-    st = f64 ? volume_from_f64(ctx, stage.as<double>(), v->n, dst, v->d_stats)
-             : volume_from_f32(ctx, stage.as<float>(), v->n, dst, v->d_stats);
+    st = f64 ? volume_from_f64(ctx, static_cast<double *>(stage), v->n, dst, v->d_stats)
+             : volume_from_f32(ctx, static_cast<float *>(stage), v->n, dst, v->d_stats);
   if (!st && bf16) st = volume_to_bf16(ctx, dst, v->n, v->d_vol16, v->d_stats);
-  if (!st) st = volume_finish_upload(v);  // also keeps the staging buffer alive until done
+  if (!st) st = volume_finish_upload(v);
   return st;
 }
 
@@ -491,10 +520,24 @@ int wrt_grid_create(wrt_ctx *ctx, int nphi, int ntheta, int nshift, wrt_grid **o
   if (!st) st = ctx_alloc(ctx, (void **)&g->d_shift, sizeof(double) * nshift);
   if (!st) st = ctx_alloc(ctx, (void **)&g->d_dir32, sizeof(float) * dir32.size());
   if (!st) st = ctx_alloc(ctx, (void **)&g->d_shift32, sizeof(float) * nshift);
+  std::vector<double> cs(2 * (size_t)ntheta);
+  std::vector<double4> dirw(ndir);
+  if (!st) {
+    for (int i = 0; i < ntheta; ++i) {
+      cs[2 * i] = cos(g->theta[i]);  // slicing.c:104-105 evaluate cos/sin(p_theta)
+      cs[2 * i + 1] = sin(g->theta[i]);
+    }
+    adjoint_directions(nphi, ntheta, nshift, g->phi.data(), g->theta.data(), g->w.data(),
+                       dirw.data());
+    st = ctx_alloc(ctx, (void **)&g->d_cs, sizeof(double) * cs.size());
+  }
+  if (!st) st = ctx_alloc(ctx, (void **)&g->d_dirw, sizeof(double4) * ndir);
   if (!st) st = h2d(ctx, g->d_dir, dir.data(), sizeof(double) * dir.size(), "grid upload");
   if (!st) st = h2d(ctx, g->d_shift, g->shift.data(), sizeof(double) * nshift, "grid upload");
   if (!st) st = h2d(ctx, g->d_dir32, dir32.data(), sizeof(float) * dir32.size(), "grid upload");
   if (!st) st = h2d(ctx, g->d_shift32, shift32.data(), sizeof(float) * nshift, "grid upload");
+  if (!st) st = h2d(ctx, g->d_cs, cs.data(), sizeof(double) * cs.size(), "grid upload");
+  if (!st) st = h2d(ctx, g->d_dirw, dirw.data(), sizeof(double4) * ndir, "grid upload");
   if (!st) {
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) st = cuda_fail(ctx, e, "grid upload");
@@ -516,6 +559,8 @@ int wrt_grid_destroy(wrt_grid *g) {
   ctx_free(g->ctx, g->d_shift, sizeof(double) * g->nshift);
   ctx_free(g->ctx, g->d_dir32, sizeof(float) * 8 * ndir);
   ctx_free(g->ctx, g->d_shift32, sizeof(float) * g->nshift);
+  ctx_free(g->ctx, g->d_cs, sizeof(double) * 2 * g->ntheta);
+  ctx_free(g->ctx, g->d_dirw, sizeof(double4) * ndir);
   delete g;
   return WRT_OK;
 }
@@ -721,24 +766,58 @@ int wrt_tune_plane_kernel(wrt_ctx *ctx, const wrt_volume *vol, const wrt_grid *g
 }
 
 // -------------------------------------------------------- drop-in, host I/O
+}  // extern "C"
+
+namespace {
+
+// The drop-in entry points keep the volume and the sphere grid of their last
+// call in the context and their buffers in its workspace, so a warm call of
+// the same sizes allocates no device memory.
+int dropin_volume(wrt_ctx *ctx, int n, const double *host, wrt_volume **out) {
+  if (ctx->dropin_vol && ctx->dropin_vol->n != n) {
+    wrt_volume_destroy(ctx->dropin_vol);
+    ctx->dropin_vol = nullptr;
+  }
+  int st = WRT_OK;
+  if (!ctx->dropin_vol) st = wrt_volume_create(ctx, n, &ctx->dropin_vol);
+  if (!st) st = wrt_volume_upload(ctx->dropin_vol, host, nullptr);
+  *out = ctx->dropin_vol;
+  return st;
+}
+
+int dropin_grid(wrt_ctx *ctx, int nphi, int ntheta, int nshift, wrt_grid **out) {
+  wrt_grid *g = ctx->dropin_grid;
+  if (g && (g->nphi != nphi || g->ntheta != ntheta || g->nshift != nshift)) {
+    wrt_grid_destroy(g);
+    ctx->dropin_grid = g = nullptr;
+  }
+  int st = WRT_OK;
+  if (!g) st = wrt_grid_create(ctx, nphi, ntheta, nshift, &ctx->dropin_grid);
+  *out = ctx->dropin_grid;
+  return st;
+}
+
+}  // namespace
+
+extern "C" {
+
 int wrt_radon_grid(wrt_ctx *ctx, const double *volume, int n, int nphi, int ntheta, int nshift,
                    const wrt_plane_opts *opts, double *out) {
   if (!ctx || !volume || !out || n < 2 || nphi < 1 || ntheta < 1 || nshift < 2)
     return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon_grid: bad arguments")
                : WRT_ERR_INVALID_ARGUMENT;
   if (!valid_plane_opts(opts, n)) return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "invalid plane options");
+  int st = set_device(ctx);
+  if (st) return st;
   wrt_volume *vol = nullptr;
   wrt_grid *grid = nullptr;
-  int st = wrt_volume_create(ctx, n, &vol);
-  if (!st) st = wrt_volume_upload(vol, volume, nullptr);
-  if (!st) st = wrt_grid_create(ctx, nphi, ntheta, nshift, &grid);
-  DevBuf dout(ctx);
+  void *dout = nullptr;
   const size_t nout = (size_t)nphi * ntheta * nshift;
-  if (!st) st = dout.alloc(sizeof(double) * nout);
-  if (!st) st = wrt_radon_forward_device(ctx, vol, grid, opts, dout.as<double>());
-  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "radon_grid result");
-  if (grid) wrt_grid_destroy(grid);
-  if (vol) wrt_volume_destroy(vol);
+  st = dropin_volume(ctx, n, volume, &vol);
+  if (!st) st = dropin_grid(ctx, nphi, ntheta, nshift, &grid);
+  if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
+  if (!st) st = wrt_radon_forward_device(ctx, vol, grid, opts, static_cast<double *>(dout));
+  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "radon_grid result");
   return st;
 }
 
@@ -778,16 +857,20 @@ int wrt_radon_transpose(wrt_ctx *ctx, const double *g, int n, int nphi, int nthe
   return st;
 }
 
-int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int n, int nslices, int nshift, int nphi,
-                 const double *frame, double *out) {
-  if (!ctx || !volume || !out || n < 2 || nslices < 2 || nshift < 2 || nphi < 1)
-    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "ray_grid: bad arguments")
+int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const double *frame,
+                           int nslices, int nshift, int nphi, double *dev_out) {
+  wrt_volume *vol = const_cast<wrt_volume *>(cvol);
+  if (!ctx || !vol || !dev_out || vol->ctx != ctx || nslices < 2 || nshift < 2 || nphi < 1)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "ray_forward_device: bad arguments")
                : WRT_ERR_INVALID_ARGUMENT;
-  wrt_volume *vol = nullptr;
-  int st = wrt_volume_create(ctx, n, &vol);
-  if (!st) st = wrt_volume_upload(vol, volume, nullptr);
+  if (vol->storage != WRT_STORAGE_F32)
+    return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "ray transform: FP32 volumes only");
+  int st = set_device(ctx);
+  if (st) return st;
+  const int n = vol->n;
   // ray_grid/src/init.c:163-176 and the trig of ray_grid/src/integral.c:16-24
-  std::vector<double> shift(nshift), trig(4 * (size_t)nphi);
+  std::vector<double> tab((size_t)nshift + 4 * (size_t)nphi);
+  double *shift = tab.data(), *trig = tab.data() + nshift;
   const double dshift = 2.0 / (nshift - 1);
   for (int i = 0; i < nshift; ++i) shift[i] = (-1.0) + i * dshift;
   const double dphi = (2 * M_PI) / nphi;
@@ -801,39 +884,61 @@ int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int n, int nslices, int nsh
   const bool identity = !frame || (frame[0] == 1.0 && frame[4] == 1.0 && frame[8] == 1.0 &&
                                    frame[1] == 0.0 && frame[2] == 0.0 && frame[3] == 0.0 &&
                                    frame[5] == 0.0 && frame[6] == 0.0 && frame[7] == 0.0);
-  DevBuf dshiftb(ctx), dtrig(ctx), dframe(ctx), dout(ctx);
-  const size_t nout = (size_t)nslices * nshift * nphi;
-  if (!st) st = dshiftb.alloc(sizeof(double) * nshift);
-  if (!st) st = dtrig.alloc(sizeof(double) * trig.size());
-  if (!st && !identity) st = dframe.alloc(sizeof(double) * 9);
-  if (!st) st = dout.alloc(sizeof(double) * nout);
-  if (!st) st = h2d(ctx, dshiftb.p, shift.data(), sizeof(double) * nshift, "ray grid");
-  if (!st) st = h2d(ctx, dtrig.p, trig.data(), sizeof(double) * trig.size(), "ray grid");
-  if (!st && !identity) st = h2d(ctx, dframe.p, frame, sizeof(double) * 9, "ray frame");
-  if (!st) {
-    RayJob job = {};
-    job.vol = vol->d_vol;
-    job.n = n;
-    job.nslices = nslices;
-    job.nshift = nshift;
-    job.nphi = nphi;
-    job.trig = dtrig.as<double>();
-    job.shift = dshiftb.as<double>();
-    job.frame = identity ? nullptr : dframe.as<double>();
-    job.r2bits = vol->d_stats;
-    job.margin = sampler_margin(n, WRT_SAMPLER_TRILINEAR);
-    job.out = dout.as<double>();
-    // z-slices read one layer pair each: build the volume's layer pairs
-    if (identity) st = volume_ensure_pairs(vol);
-    if (!st && identity) {
-      job.pairs = vol->d_pairs;
-      job.pitch = vol->pitch;
-    }
-    if (!st) st = ray_forward(ctx, job);
+  void *dtab = nullptr;
+  st = ws_get(ctx, WS_TABLE, sizeof(double) * tab.size(), &dtab);
+  // a copy from pageable memory returns once the data is staged
+  if (!st) st = h2d(ctx, dtab, tab.data(), sizeof(double) * tab.size(), "ray grid");
+  // z-slices read one layer pair each: the volume's layer pairs (built once)
+  if (!st && identity) st = volume_ensure_pairs(vol);
+  if (st) return st;
+  RayJob job = {};
+  job.vol = vol->d_vol;
+  job.n = n;
+  job.nslices = nslices;
+  job.nshift = nshift;
+  job.nphi = nphi;
+  job.shift = static_cast<const double *>(dtab);
+  job.trig = static_cast<const double *>(dtab) + nshift;
+  job.has_frame = identity ? 0 : 1;
+  if (!identity)
+    for (int k = 0; k < 9; ++k) job.frame[k] = frame[k];
+  job.r2bits = vol->d_stats;
+  job.margin = sampler_margin(n, WRT_SAMPLER_TRILINEAR);
+  job.out = dev_out;
+  if (identity) {
+    job.pairs = vol->d_pairs;
+    job.pitch = vol->pitch;
   }
-  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "ray_grid result");
-  if (vol) wrt_volume_destroy(vol);
+  return ray_forward(ctx, job);
+}
+
+int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int n, int nslices, int nshift, int nphi,
+                 const double *frame, double *out) {
+  if (!ctx || !volume || !out || n < 2 || nslices < 2 || nshift < 2 || nphi < 1)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "ray_grid: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  if (st) return st;
+  wrt_volume *vol = nullptr;
+  void *dout = nullptr;
+  const size_t nout = (size_t)nslices * nshift * nphi;
+  st = dropin_volume(ctx, n, volume, &vol);
+  if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
+  if (!st) st = wrt_ray_forward_device(ctx, vol, frame, nslices, nshift, nphi,
+                                       static_cast<double *>(dout));
+  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "ray_grid result");
   return st;
+}
+
+int wrt_radon_reduction_device(wrt_ctx *ctx, const double *dev_rays, int ngrid, int nshift_ray,
+                               const wrt_grid *grid, double *dev_out) {
+  if (!ctx || !dev_rays || !grid || !dev_out || grid->ctx != ctx || ngrid < 3 || nshift_ray < 3)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon_reduction_device: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  if (st) return st;
+  return reduction_forward(ctx, dev_rays, ngrid, nshift_ray, grid->nphi, grid->d_shift,
+                           grid->nshift, grid->d_cs, grid->ntheta, dev_out);
 }
 
 int wrt_radon_reduction(wrt_ctx *ctx, const double *rays, int ngrid, int nshift_ray, int nphi,
@@ -843,52 +948,50 @@ int wrt_radon_reduction(wrt_ctx *ctx, const double *rays, int ngrid, int nshift_
                : WRT_ERR_INVALID_ARGUMENT;
   int st = set_device(ctx);
   if (st) return st;
-  std::vector<double> phi(nphi), theta(ntheta), w(ntheta), shift(nshift);
-  st = sphere_grid(ctx, nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), shift.data());
-  std::vector<double> cs(2 * (size_t)ntheta);
-  for (int i = 0; i < ntheta; ++i) {
-    cs[2 * i] = cos(theta[i]);  // slicing.c:104-105 evaluate cos/sin(p_theta)
-    cs[2 * i + 1] = sin(theta[i]);
-  }
-  DevBuf drays(ctx), dshift(ctx), dcs(ctx), dout(ctx);
+  wrt_grid *grid = nullptr;
+  void *din = nullptr, *dout = nullptr;
   const size_t nin = (size_t)ngrid * nshift_ray * nphi, nout = (size_t)nshift * nphi * ntheta;
-  if (!st) st = drays.alloc(sizeof(double) * nin);
-  if (!st) st = dshift.alloc(sizeof(double) * nshift);
-  if (!st) st = dcs.alloc(sizeof(double) * cs.size());
-  if (!st) st = dout.alloc(sizeof(double) * nout);
-  if (!st) st = h2d(ctx, drays.p, rays, sizeof(double) * nin, "reduction input");
-  if (!st) st = h2d(ctx, dshift.p, shift.data(), sizeof(double) * nshift, "reduction grid");
-  if (!st) st = h2d(ctx, dcs.p, cs.data(), sizeof(double) * cs.size(), "reduction grid");
+  st = dropin_grid(ctx, nphi, ntheta, nshift, &grid);
+  if (!st) st = ws_get(ctx, WS_IN, sizeof(double) * nin, &din);
+  if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
+  if (!st) st = h2d(ctx, din, rays, sizeof(double) * nin, "reduction input");
   if (!st)
-    st = reduction_forward(ctx, drays.as<double>(), ngrid, nshift_ray, nphi, dshift.as<double>(),
-                           nshift, dcs.as<double>(), ntheta, dout.as<double>());
-  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "reduction result");
+    st = wrt_radon_reduction_device(ctx, static_cast<const double *>(din), ngrid, nshift_ray, grid,
+                                    static_cast<double *>(dout));
+  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "reduction result");
   return st;
+}
+
+int wrt_radon3d_adjoint_device(wrt_ctx *ctx, const double *dev_radon, const wrt_grid *grid,
+                               int ngrid, double *dev_out) {
+  if (!ctx || !dev_radon || !grid || !dev_out || grid->ctx != ctx || ngrid < 1 || ngrid > 4096 ||
+      grid->nshift < 3)
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon3d_adjoint_device: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
+  int st = set_device(ctx);
+  if (st) return st;
+  return adjoint_forward(ctx, dev_radon, grid->nphi, grid->ntheta, grid->nshift, grid->d_dirw,
+                         ngrid, dev_out);
 }
 
 int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta, int nshift,
                         int ngrid, double *out) {
-  if (!ctx || !radon || !out || ngrid < 1 || nphi < 1 || ntheta < 1 || nshift < 3)
+  if (!ctx || !radon || !out || ngrid < 1 || ngrid > 4096 || nphi < 1 || ntheta < 1 || nshift < 3)
     return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon3d_adjoint: bad arguments")
                : WRT_ERR_INVALID_ARGUMENT;
   int st = set_device(ctx);
   if (st) return st;
-  std::vector<double> phi(nphi), theta(ntheta), w(ntheta), shift(nshift);
-  st = sphere_grid(ctx, nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), shift.data());
-  const int ndir = nphi * ntheta;
-  std::vector<double4> dirw(ndir);
-  adjoint_directions(nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), dirw.data());
-  DevBuf dradon(ctx), ddirw(ctx), dout(ctx);
-  const size_t nin = (size_t)nshift * ndir, nout = (size_t)ngrid * ngrid * ngrid;
-  if (!st) st = dradon.alloc(sizeof(double) * nin);
-  if (!st) st = ddirw.alloc(sizeof(double4) * ndir);
-  if (!st) st = dout.alloc(sizeof(double) * nout);
-  if (!st) st = h2d(ctx, dradon.p, radon, sizeof(double) * nin, "adjoint input");
-  if (!st) st = h2d(ctx, ddirw.p, dirw.data(), sizeof(double4) * ndir, "adjoint directions");
+  wrt_grid *grid = nullptr;
+  void *din = nullptr, *dout = nullptr;
+  const size_t nin = (size_t)nshift * nphi * ntheta, nout = (size_t)ngrid * ngrid * ngrid;
+  st = dropin_grid(ctx, nphi, ntheta, nshift, &grid);
+  if (!st) st = ws_get(ctx, WS_IN, sizeof(double) * nin, &din);
+  if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
+  if (!st) st = h2d(ctx, din, radon, sizeof(double) * nin, "adjoint input");
   if (!st)
-    st = adjoint_forward(ctx, dradon.as<double>(), nphi, ntheta, nshift, ddirw.as<double4>(), ngrid,
-                         dout.as<double>());
-  if (!st) st = d2h_sync(ctx, out, dout.p, sizeof(double) * nout, "adjoint result");
+    st = wrt_radon3d_adjoint_device(ctx, static_cast<const double *>(din), grid, ngrid,
+                                    static_cast<double *>(dout));
+  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "adjoint result");
   return st;
 }
 

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) 
   }
   const double h = 0.5 * (n - 1);
   const float qmax = (float)(n - 1);
-  const double *F = job.frame;
+  const double *F = job.frame;  // kernel parameter space
   if (any && !FRAME) {
     any = clip_axis(p0x, ax, klo, khi) && clip_axis(p0y, ay, klo, khi) && fabs(zslice) <= 1.0;
   } else if (any) {
@@ -197,7 +197,7 @@ int ray_forward(wrt_ctx *ctx, const RayJob &job) {
   const long long blocks = (nrays + 255) / 256;
   if (blocks > 0x7fffffffLL) return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "too many rays");
   const float g = 4.8e-7f * (float)(job.n > 64 ? job.n : 64);
-  if (job.frame)
+  if (job.has_frame)
     ray_kernel<true><<<(unsigned)blocks, 256, 0, ctx->stream>>>(job, g);
   else
     ray_kernel<false><<<(unsigned)blocks, 256, 0, ctx->stream>>>(job, g);

@@ -114,53 +114,37 @@ __global__ void __launch_bounds__(256, 3)
 
 unsigned adjoint_blocks(int n) { return (unsigned)((wrtd::adjoint_warps(n) + 7) / 8); }
 
+// Natural splines of nlines lines into the context's workspace (records in
+// WS_LINES); asynchronous on the context's stream.
 int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long long so,
-               long long se, long long si, int ns, float4 **d_lines, size_t *bytes,
+               long long se, long long si, int ns, float4 **d_lines,
                const double4 *d_weights) {
   // line-independent elimination coefficients for the uniform-knot system
   // h M_{i-1} + 4h M_i + h M_{i+1} = rhs (divided by h: M_{i-1} + 4 M_i + M_{i+1})
   const double h = 2.0 / (ns - 1);
-  std::vector<double> cp(ns, 0.0), den(ns, 1.0);
+  std::vector<double> coef(2 * (size_t)ns, 0.0);
+  double *cp = coef.data(), *den = coef.data() + ns;
+  for (int i = 0; i < ns; ++i) den[i] = 1.0;
   for (int i = 1; i + 1 < ns; ++i) {
     den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);
     cp[i] = 1.0 / den[i];
   }
-  // the kernel divides rhs by den and uses cp; rhs is 6/h^2 * second difference
-  double *d_coef = nullptr, *d_scratch = nullptr;
-  int st = wrt::ctx_alloc(ctx, (void **)&d_coef, sizeof(double) * 2 * ns);
+  void *d_coef = nullptr, *d_scratch = nullptr, *lines = nullptr;
+  int st = wrt::ws_get(ctx, wrt::WS_COEF, sizeof(double) * coef.size(), &d_coef);
+  if (!st) st = wrt::ws_get(ctx, wrt::WS_SPLINE, sizeof(double) * (size_t)nlines * ns, &d_scratch);
+  if (!st) st = wrt::ws_get(ctx, wrt::WS_LINES, sizeof(float4) * (size_t)nlines * (ns - 1), &lines);
   if (st) return st;
-  const size_t scratch_bytes = sizeof(double) * (size_t)nlines * ns;
-  st = wrt::ctx_alloc(ctx, (void **)&d_scratch, scratch_bytes);
-  if (st) {
-    wrt::ctx_free(ctx, d_coef, sizeof(double) * 2 * ns);
-    return st;
-  }
-  *bytes = sizeof(float4) * (size_t)nlines * (ns - 1);
-  st = wrt::ctx_alloc(ctx, (void **)d_lines, *bytes);
-  if (!st) {
-    cudaError_t e = cudaMemcpyAsync(d_coef, cp.data(), sizeof(double) * ns,
-                                    cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(d_coef + ns, den.data(), sizeof(double) * ns, cudaMemcpyHostToDevice,
-                          ctx->stream);
-    if (e != cudaSuccess) {
-      st = wrt::cuda_fail(ctx, e, "spline coefficients");
-    } else {
-      spline_prep_kernel<<<(nlines + 127) / 128, 128, 0, ctx->stream>>>(
-          d_src, nlines, ninner, so, se, si, ns, h, d_coef, d_coef + ns, d_scratch, *d_lines,
-          d_weights);
-      ctx->launches++;
-      st = wrt::check_launch(ctx, "spline_prep_kernel");
-      if (!st) {
-        e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) st = wrt::cuda_fail(ctx, e, "spline prep");
-      }
-    }
-    if (st) wrt::ctx_free(ctx, *d_lines, *bytes);
-  }
-  wrt::ctx_free(ctx, d_scratch, scratch_bytes);
-  wrt::ctx_free(ctx, d_coef, sizeof(double) * 2 * ns);
-  return st;
+  // a copy from pageable memory returns once the data is staged
+  cudaError_t e = cudaMemcpyAsync(d_coef, coef.data(), sizeof(double) * coef.size(),
+                                  cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "spline coefficients");
+  const double *dc = static_cast<const double *>(d_coef);
+  *d_lines = static_cast<float4 *>(lines);
+  spline_prep_kernel<<<(nlines + 127) / 128, 128, 0, ctx->stream>>>(
+      d_src, nlines, ninner, so, se, si, ns, h, dc, dc + ns, static_cast<double *>(d_scratch),
+      *d_lines, d_weights);
+  ctx->launches++;
+  return wrt::check_launch(ctx, "spline_prep_kernel");
 }
 
 }  // namespace
@@ -190,43 +174,28 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
                       double *d_out) {
   // lines (iz, iphi): element is at d_rays[(iz*ns_ray + is)*nphi + iphi]
   float4 *d_lines = nullptr;
-  size_t bytes = 0;
   int st = prep_lines(ctx, d_rays, ngrid * nphi, nphi, (long long)nshift_ray * nphi, nphi, 1,
-                      nshift_ray, &d_lines, &bytes, nullptr);
+                      nshift_ray, &d_lines, nullptr);
   if (st) return st;
   const long long total = (long long)nshift * nphi * ntheta;
   const long long blocks = (total + 255) / 256;
   reduction_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(d_lines, ngrid, nshift_ray, nphi,
                                                               d_shift, nshift, d_cs, ntheta, d_out);
   ctx->launches++;
-  st = check_launch(ctx, "reduction_kernel");
-  if (!st) {
-    cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) st = cuda_fail(ctx, e, "reduction");
-  }
-  ctx_free(ctx, d_lines, bytes);
-  return st;
+  return check_launch(ctx, "reduction_kernel");
 }
 
 int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
                     const double4 *d_dirw, int n, double *d_out) {
   // lines (iphi, itheta): element is at d_radon[(is*nphi + iphi)*ntheta + itheta]
   float4 *d_lines = nullptr;
-  size_t bytes = 0;
   const int ndir = nphi * ntheta;
-  int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, &bytes,
-                      d_dirw);
+  int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, d_dirw);
   if (st) return st;
   adjoint_kernel<<<adjoint_blocks(n), 256, 0, ctx->stream>>>(d_lines, ndir, nshift, d_dirw, n,
                                                               d_out);
   ctx->launches++;
-  st = check_launch(ctx, "adjoint_kernel");
-  if (!st) {
-    cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) st = cuda_fail(ctx, e, "adjoint");
-  }
-  ctx_free(ctx, d_lines, bytes);
-  return st;
+  return check_launch(ctx, "adjoint_kernel");
 }
 
 }  // namespace wrt

@@ -56,6 +56,14 @@ struct wrt_ctx {
   void *staged_cache = nullptr;
   int staged_config = -1;  // tile configuration (-1: default), set by the autotuner
   void *batch_slot = nullptr;  // BatchSlot of wrt_radon_forward_batch (batch.cu)
+  // grow-only working buffers, one per role (wrt::ws_get), freed with the
+  // context: warm calls of the same or smaller sizes allocate nothing
+  void *ws[8] = {};
+  size_t ws_bytes[8] = {};
+  // the volume and sphere grid of the last drop-in (host-array) call, kept
+  // for the next call of the same sizes
+  wrt_volume *dropin_vol = nullptr;
+  wrt_grid *dropin_grid = nullptr;
 };
 
 namespace wrt {
@@ -66,6 +74,10 @@ int cuda_fail(wrt_ctx *ctx, cudaError_t e, const char *what);
 int ctx_alloc(wrt_ctx *ctx, void **p, size_t bytes);
 void ctx_free(wrt_ctx *ctx, void *p, size_t bytes);
 int check_launch(wrt_ctx *ctx, const char *what);
+// Working buffer of a role, at least `bytes` long (grown after the context's
+// stream has drained; contents are not kept).
+enum WsRole { WS_STAGE, WS_IN, WS_OUT, WS_LINES, WS_SPLINE, WS_COEF, WS_TABLE, WS_ROLES };
+int ws_get(wrt_ctx *ctx, int role, size_t bytes, void **p);
 
 // Host-side FP64 geometry, computed with the host libm exactly as the
 // reference computes it (radon_grid/src/integral.c:10-36).
@@ -257,7 +269,8 @@ struct RayJob {
   int nslices, nshift, nphi;
   const double *trig;   // [nphi][4]: cos phi, sin phi, cos(phi+pi/2), sin(phi+pi/2)
   const double *shift;  // [nshift]
-  const double *frame;  // 9 doubles on the device, or null for the z-slices
+  double frame[9];      // row-major rotation of the sample points (has_frame)
+  int has_frame;        // 0: the reference's z-slices
   const unsigned int *r2bits;
   double margin;
   double *out;          // [nslices][nshift][nphi]
