@@ -240,6 +240,214 @@ def run_reference(args, dist):
     return 0
 
 
+# ------------------------------------------------------------ the other hot paths
+RAY_SLICES, RAY_SHIFTS, RAY_PHIS = 128, 128, 128
+
+
+def rotated_frame(seed):
+    rng = np.random.default_rng(seed)
+    q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+    frame = q * np.sign(np.diag(r))
+    if np.linalg.det(frame) < 0:
+        frame[:, 0] = -frame[:, 0]
+    return frame
+
+
+def timed_device_calls(ctx, call, steps, warmup):
+    """CUDA-event times (ms) of `call` on the library's stream, L2 flushed
+    before each timed call."""
+    for _ in range(max(warmup, 3)):
+        call()
+    ctx.synchronize()
+    times = []
+    for _ in range(steps):
+        ctx.flush_l2()
+        ctx.timer_start()
+        call()
+        times.append(ctx.timer_stop())
+    return times
+
+
+def other_paths(wrt, ctx, phantom, steps, warmup, smem_bw, with_cpu):
+    """The ray transform (reference frame and one rotated frame), the
+    reduction of ray data to Radon data, and the backprojection, at 128^3,
+    through their device-resident entry points: device time per call, units/s,
+    the gather roofline of the dominant kernel (bytes per counted unit against
+    the measured shared-memory/L1 bandwidth) and, in the CPU leg, the
+    reference's own code on a bounded seeded sample of the same units, timed
+    on the host cores and compared with the GPU's values there."""
+    n = N
+    vol = wrt.Volume(ctx, n)
+    vol.upload(phantom.astype(np.float32))
+    grid = wrt.Grid(ctx, NPHI, NTHETA, NSHIFT)
+    nrays = RAY_SLICES * RAY_SHIFTS * RAY_PHIS
+    rays_d = wrt.DeviceBuffer(ctx, nrays * 8)
+    radon_d = wrt.DeviceBuffer(ctx, grid.nplanes * 8)
+    adj_d = wrt.DeviceBuffer(ctx, n ** 3 * 8)
+    frame = rotated_frame(SEED)
+    rng = np.random.default_rng(SEED + 7)
+    gauss = rng.standard_normal((NSHIFT, NPHI, NTHETA))
+    res = {}
+
+    def counted(call):
+        ctx.count_samples(True)
+        call()
+        c = ctx.sample_count()
+        ctx.count_samples(False)
+        return c
+
+    def entry(name, call, units, unit, bytes_per_sample, samples, sample_unit, download):
+        times = timed_device_calls(ctx, call, steps, warmup)
+        ms = statistics.mean(times)
+        achieved = samples * bytes_per_sample / (ms * 1e-3) / 1e9
+        res[name] = {"value": units / (ms * 1e-3), "unit": unit, "ms_per_call": ms,
+                     "ms_median": statistics.median(times), "gpu_launches_per_call": None,
+                     "roofline": {"bound": "l1tex", "achieved": achieved, "peak": smem_bw / 1e9,
+                                  "unit": "GB/s", "frac": achieved / (smem_bw / 1e9),
+                                  "algorithmic_bytes": f"{bytes_per_sample} B per {sample_unit}",
+                                  "samples_per_call": samples}}
+        return download()
+
+    ray_call = lambda fr=None: wrt.ray_forward_device(ctx, vol, RAY_SLICES, RAY_SHIFTS, RAY_PHIS,
+                                                       rays_d.ptr, frame=fr)
+    dl_rays = lambda: rays_d.download(np.empty((RAY_SLICES, RAY_SHIFTS, RAY_PHIS)))
+    l0 = ctx.launches
+    rays = entry("ray", ray_call, nrays, "rays/s", BYTES_PER_SAMPLE, counted(ray_call),
+                 "trilinear sample (8 FP32 corners)", dl_rays)
+    res["ray"]["gpu_launches_per_call"] = (ctx.launches - l0) // (steps + max(warmup, 3) + 1)
+    rc = lambda: ray_call(frame)
+    rays_rot = entry("ray_rotated", rc, nrays, "rays/s", BYTES_PER_SAMPLE, counted(rc),
+                     "trilinear sample (8 FP32 corners)", dl_rays)
+    # the reduction reads the reference-frame rays (128 offsets) from the device
+    ray_call()
+    red = lambda: wrt.radon_reduction_device(ctx, rays_d.ptr, n, RAY_SHIFTS, grid, radon_d.ptr)
+    radon = entry("reduction", red, grid.nplanes, "plane integrals/s", 48, counted(red),
+                  "slice sample (3 spline records of 16 B)",
+                  lambda: radon_d.download(np.empty((NSHIFT, NPHI, NTHETA))))
+    gauss_d = wrt.DeviceBuffer(ctx, gauss.nbytes)
+    gauss_d.upload(gauss)
+    adj = lambda: wrt.radon3d_adjoint_device(ctx, gauss_d.ptr, grid, n, adj_d.ptr)
+    evals = n ** 3 * NPHI * NTHETA
+    adjoint = entry("adjoint", adj, n ** 3, "voxels/s", 16, evals,
+                    "spline evaluation (one 16 B record)",
+                    lambda: adj_d.download(np.empty((n, n, n))))
+    for k, w in (("ray", "128^3, 128 layers x 128 shifts x 128 angles, reference frame"),
+                 ("ray_rotated", "the same in one seeded rotated layer frame"),
+                 ("reduction", "128^3 rays (128 offsets) -> 64x128 sphere grid x 256 shifts"),
+                 ("adjoint", "N(0,1) Radon data 64x128x256 -> 128^3 voxels")):
+        res[k]["workload"] = w
+    if with_cpu:
+        import oracle as O
+        cores = cpu_threads()
+        ref = O.Reference() if O.Reference.available() else None
+        s_grid, phi_grid = O.ray_grid(RAY_SHIFTS, RAY_PHIS)
+        # ray: the reference's ray_transform on 16384 seeded rays
+        m = 16384
+        idx = rng.integers(0, nrays, size=m)
+        iz, i_s, ip = idx // (RAY_SHIFTS * RAY_PHIS), (idx // RAY_PHIS) % RAY_SHIFTS, idx % RAY_PHIS
+        z = -1.0 + iz * (2.0 / (RAY_SLICES - 1))
+        if ref:
+            t0 = time.perf_counter()
+            got = ref.rays(phantom, z, s_grid[i_s], phi_grid[ip], cores)
+            wall = time.perf_counter() - t0
+            res["ray"]["cpu_baseline"] = {
+                "value": m / wall, "unit": "rays/s", "cores": cores, "kind": "reference",
+                "sample": f"{m} seeded rays, ray_grid's ray_transform (oracle/_ref), FP64"}
+            res["ray"]["rel_l2_vs_reference_on_sample"] = float(
+                np.linalg.norm(rays.reshape(-1)[idx] - got) / np.linalg.norm(got))
+        # rotated frame: the FP64 restatement (the reference has no layer frames)
+        m = 1024
+        idx = idx[:m]
+        t0 = time.perf_counter()
+        got = np.array([O.ray_transform(phantom, a, s_grid[b], phi_grid[c], frame=frame)
+                        for a, b, c in zip(z[:m], i_s[:m], ip[:m])])
+        wall = time.perf_counter() - t0
+        res["ray_rotated"]["cpu_baseline"] = {
+            "value": m / wall, "unit": "rays/s", "cores": 1, "kind": "port",
+            "sample": f"{m} seeded rays, FP64 oracle restatement with the frame, one thread"}
+        res["ray_rotated"]["rel_l2_vs_oracle_on_sample"] = float(
+            np.linalg.norm(rays_rot.reshape(-1)[idx] - got) / np.linalg.norm(got))
+        # reduction: the restatement on 2048 seeded planes (decoupled shift grids);
+        # the reference itself on coupled grids (its own definition) for the timing
+        m = 2048
+        sel = rng.integers(0, [NSHIFT, NPHI, NTHETA], size=(m, 3))
+        got = O.reduction_planes(rays[:n], NSHIFT, NTHETA, sel[:, 0], sel[:, 1], sel[:, 2],
+                                 nthreads=cores)
+        res["reduction"]["rel_l2_vs_oracle_on_sample"] = float(
+            np.linalg.norm(radon[sel[:, 0], sel[:, 1], sel[:, 2]] - got) / np.linalg.norm(got))
+        if ref:
+            rays_c = ctx.ray_grid(phantom, n, NSHIFT, RAY_PHIS)
+            t0 = time.perf_counter()
+            ref.reduction_planes(rays_c, NTHETA, sel[:, 0], sel[:, 1], sel[:, 2], cores)
+            wall = time.perf_counter() - t0
+            res["reduction"]["cpu_baseline"] = {
+                "value": m / wall, "unit": "plane integrals/s", "cores": cores,
+                "kind": "reference",
+                "sample": f"{m} seeded planes, radon_reduction's radon_reduction (oracle/_ref) "
+                          "on rays with 256 offsets (the reference couples the shift grids)"}
+        # adjoint: the reference's radon3d_adjoint at 128 seeded voxels
+        m = 128
+        idx = rng.integers(0, n ** 3, size=m)
+        a, b, c = idx // (n * n), (idx // n) % n, idx % n  # [iz][ix][iy]
+        ctr = lambda i: -1.0 + (2.0 * i + 1.0) / n
+        if ref:
+            t0 = time.perf_counter()
+            got = ref.adjoint_points(gauss, ctr(b), ctr(c), ctr(a), cores)
+            wall = time.perf_counter() - t0
+            res["adjoint"]["cpu_baseline"] = {
+                "value": m / wall, "unit": "voxels/s", "cores": cores, "kind": "reference",
+                "sample": f"{m} seeded voxels, the backprojection's radon3d_adjoint (oracle/_ref)"}
+            res["adjoint"]["rel_l2_vs_reference_on_sample"] = float(
+                np.linalg.norm(adjoint.reshape(-1)[idx] - got) / np.linalg.norm(got))
+    for b in (rays_d, radon_d, adj_d, gauss_d):
+        b.close()
+    grid.close()
+    vol.close()
+    return res
+
+
+def batch_vs_one_per_launch(wrt, ctx, steps):
+    """64 FP32 volumes of uneven edge lengths {48..192}, each with its own
+    sphere grid (16-96 latitudes x twice as many longitudes, 64-256 shifts):
+    all in ONE graph-captured launch of the persistent kernel
+    (wrt_radon_forward_batch) against the same 64 requests run one
+    wrt_radon_forward_device call (staged kernel) per request.  Device time
+    with CUDA events, L2 flushed before each timed run."""
+    from wrt_b200.phantom import ellipsoid_phantom
+
+    rng = np.random.default_rng(2002)
+    reqs, keep, planes = [], [], 0
+    for k in range(64):
+        n = int(rng.choice([48, 64, 96, 128, 160, 192]))
+        nth = int(rng.integers(16, 97))
+        ns = int(rng.integers(64, 257))
+        v = wrt.Volume(ctx, n)
+        v.upload(ellipsoid_phantom(n, int(rng.integers(4, 25)), 3000 + k).astype(np.float32))
+        g = wrt.Grid(ctx, 2 * nth, nth, ns)
+        out = wrt.DeviceBuffer(ctx, g.nplanes * 8)
+        reqs.append((v, g, out.ptr, n))
+        keep.append((v, g, out))
+        planes += g.nplanes
+    batched = lambda: wrt.radon_forward_batch(ctx, reqs)
+
+    def one_by_one():
+        for v, g, ptr, n in reqs:
+            wrt.radon_forward_device(ctx, v, g, ptr, sampler=wrt.TRILINEAR, half_extent=n,
+                                     kernel=wrt.KERNEL_STAGED)
+    tb = timed_device_calls(ctx, batched, steps, 2)
+    first = [o.download(np.empty(g.nplanes)) for _, g, o in keep]
+    to = timed_device_calls(ctx, one_by_one, steps, 2)
+    same = all(np.array_equal(f, o.download(np.empty(g.nplanes)))
+               for f, (_, g, o) in zip(first, keep))
+    for v, g, o in keep:
+        o.close(); g.close(); v.close()
+    mb, mo = statistics.mean(tb), statistics.mean(to)
+    return {"requests": 64, "planes": planes, "batched_ms": mb, "one_per_launch_ms": mo,
+            "ratio": mo / mb, "batched_plane_integrals_per_s": planes / (mb * 1e-3),
+            "results_bitwise_equal": same,
+            "note": "ratio = time of 64 single-request launches / time of one batched launch"}
+
+
 # ------------------------------------------------------------ our arm
 def traffic_from_profiles():
     """DRAM bytes per launch of the plane kernel from the committed ncu summary."""
@@ -329,6 +537,149 @@ def serving_mix(wrt, dev, count, seed, budget):
             "launches": int(st.launches), "hbm_peak_bytes": int(st.bytes_peak),
             "budget_bytes": int(st.budget),
             "mean_batch": float(np.mean([i.batch_size for _, i in infos]))}
+
+
+def serving_stream(args, dist):
+    """The serving configuration at its stated size: `--requests` (10,000)
+    transform requests arriving as a seeded Poisson stream, each a volume of
+    edge 64/96/128/192/256 (w.p. .30/.25/.20/.15/.10) with a forward Radon
+    transform (80 %) or a backprojection of seeded Gaussian Radon data (20 %),
+    sphere grids of 32..96 latitudes x twice as many longitudes, 128..384
+    shifts, admitted by one wrt_server under a 60 GB HBM budget.  FP32 volumes
+    come from 4 seeded ellipsoid phantoms per edge; Radon data are windows of
+    one seeded Gaussian pool at seeded offsets.  Arrival rate: 90 % of the
+    service rate measured on 32 requests run back to back first.  Reported:
+    p50/p99 latency (submission to result in the caller's buffer), requests/s,
+    plane integrals/s, lattice samples/s and spline evaluations/s, mean batch,
+    launches, peak HBM.  One request in 100 is checked against the FP64 oracle
+    on 8 seeded planes (forward) or voxels (backprojection)."""
+    import queue
+
+    wrt = load_package()
+    from wrt_b200.phantom import ellipsoid_phantom
+
+    sys.path.insert(0, str(ROOT))
+    import oracle as O
+
+    count = args.requests
+    rng = np.random.default_rng(4000)
+    edges = rng.choice([64, 96, 128, 192, 256], size=count, p=[0.30, 0.25, 0.20, 0.15, 0.10])
+    nths = rng.integers(32, 97, size=count)
+    nss = rng.integers(128, 385, size=count)
+    fwd = rng.random(count) < 0.8
+    variant = rng.integers(0, 4, size=count)
+    pool = rng.standard_normal(16 << 20)
+    offsets = rng.integers(0, pool.size - 96 * 96 * 2 * 384, size=count)
+    vols = {(n, v): ellipsoid_phantom(n, 12, 5000 + 10 * n + v).astype(np.float32)
+            for n in (64, 96, 128, 192, 256) for v in range(4)}
+
+    def make(k):
+        n, nth, ns = int(edges[k]), int(nths[k]), int(nss[k])
+        if fwd[k]:
+            out = np.empty((ns, 2 * nth, nth))
+            return ("fwd", n, nth, ns, vols[(n, int(variant[k]))], out)
+        size = ns * 2 * nth * nth
+        radon = pool[offsets[k]:offsets[k] + size].reshape(ns, 2 * nth, nth)
+        return ("adj", n, nth, ns, radon, np.empty((n, n, n)))
+
+    def submit(srv, r, tag):
+        op, n, nth, ns, data, out = r
+        if op == "fwd":
+            return srv.submit_forward(data, 2 * nth, nth, ns, out, half_extent=n, tag=tag)
+        return srv.submit_adjoint(data, n, out, tag=tag)
+
+    checks = []
+    with wrt.Server(0, budget_bytes=60 << 30, max_batch=16, max_inflight=2) as srv:
+        # service rate: 32 requests of the same distribution back to back
+        warm = [make(k) for k in range(32)]
+        t0 = time.perf_counter()
+        ids = [submit(srv, r, 0) for r in warm]
+        for i in ids:
+            srv.wait(i)
+        service = 32 / (time.perf_counter() - t0)
+        rate = 0.9 * service
+        gaps = np.random.default_rng(4001).exponential(1.0 / rate, size=count)
+        done = queue.Queue()
+        infos = [None] * count
+
+        def waiter():
+            while True:
+                item = done.get()
+                if item is None:
+                    return
+                k, rid, r = item
+                infos[k] = srv.wait(rid)
+                if k % 100 == 0:
+                    checks.append((k, r))
+        th = threading.Thread(target=waiter, daemon=True)
+        th.start()
+        clocks = ClockSampler(0)
+        clocks.start()
+        t_start = time.perf_counter()
+        t_next = t_start
+        for k in range(count):
+            t_next += gaps[k]
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            r = make(k)
+            done.put((k, submit(srv, r, k), r))
+        done.put(None)
+        th.join()
+        wall = time.perf_counter() - t_start
+        clk = clocks.stop()
+        st = srv.stats()
+    lat = np.array([i.done_ms - i.submit_ms for i in infos])
+    queue_ms = np.array([i.start_ms - i.submit_ms for i in infos])
+    planes = int(sum(int(nss[k]) * 2 * int(nths[k]) ** 2 for k in range(count) if fwd[k]))
+    lattice = int(sum(int(nss[k]) * 2 * int(nths[k]) ** 2 * (2 * int(edges[k])) ** 2
+                      for k in range(count) if fwd[k]))
+    evals = int(sum(int(edges[k]) ** 3 * 2 * int(nths[k]) ** 2 for k in range(count) if not fwd[k]))
+    # oracle spot checks of the served results
+    errs = []
+    crng = np.random.default_rng(4002)
+    for k, (op, n, nth, ns, data, out) in sorted(checks, key=lambda c: c[0]):
+        if op == "fwd":
+            phi, theta, _, shift = O.radon_grid(2 * nth, nth, ns)
+            sel = crng.integers(0, [ns, 2 * nth, nth], size=(8, 3))
+            ref = O.radon_planes(data, phi[sel[:, 1]], theta[sel[:, 2]], shift[sel[:, 0]],
+                                 sampler=O.TRILINEAR, half_extent=n)
+            got = out[sel[:, 0], sel[:, 1], sel[:, 2]]
+        else:
+            sel = crng.integers(0, n, size=(8, 3))  # iz, ix, iy
+            c = lambda i: -1.0 + (2.0 * i + 1.0) / n
+            ref = O.adjoint_points(data, c(sel[:, 1]), c(sel[:, 2]), c(sel[:, 0]))
+            got = out[sel[:, 0], sel[:, 1], sel[:, 2]]
+        errs.append({"request": k, "op": op, "n": n, "grid": [nth, 2 * nth, ns],
+                     "rel_l2": float(np.linalg.norm(got - ref) / np.linalg.norm(ref))})
+    worst = max(e["rel_l2"] for e in errs)
+    print(json.dumps({
+        "metric": "served requests/s, 10,000-request Poisson stream (p50/p99 ms)",
+        "value": count / wall, "unit": "requests/s", "n_gpus": 1, "higher_is_better": True,
+        "path": "serving", "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving: Poisson arrivals, edge 64/96/128/192/256 w.p. "
+                               ".30/.25/.20/.15/.10, 80/20 forward/adjoint, grids 32x64..96x192, "
+                               "128-384 shifts, FP32 volumes, 60 GB HBM budget",
+                   "requests": count, "max_batch": 16, "max_inflight": 2},
+        "requests": count, "completed": int(st.completed), "failed": int(st.failed),
+        "forward": int(fwd.sum()), "adjoint": int(count - fwd.sum()),
+        "service_rate_per_s": service, "arrival_rate_per_s": rate, "wall_s": wall,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p90": float(np.percentile(lat, 90)),
+                       "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+        "queue_ms": {"p50": float(np.percentile(queue_ms, 50)),
+                     "p99": float(np.percentile(queue_ms, 99))},
+        "plane_integrals_per_s": planes / wall, "lattice_samples_per_s": lattice / wall,
+        "spline_evaluations_per_s": evals / wall,
+        "samples_definition": "forward: (2n)^2 lattice points per plane (the benchmark lattice, "
+                              "before cropping); adjoint: n^3 x directions spline evaluations",
+        "mean_batch": float(np.mean([i.batch_size for i in infos])),
+        "launches": int(st.launches), "hbm_peak_bytes": int(st.bytes_peak),
+        "budget_bytes": int(st.budget), "clocks": clk,
+        "oracle_checks": {"requests_checked": len(errs), "per_request": "8 seeded planes or voxels",
+                          "max_rel_l2": worst, "tolerance": 1e-5, "all_within": worst <= 1e-5,
+                          "median_rel_l2": float(np.median([e["rel_l2"] for e in errs])),
+                          "worst": sorted(errs, key=lambda e: -e["rel_l2"])[:3]}}))
+    return 0
 
 
 def run_ours(args, dist):
@@ -464,6 +815,10 @@ def run_ours(args, dist):
         "gpu_launches": launches,
         "roofline": {"bound": "l1tex", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic_from_profiles(),
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                       "from the committed ncu capture of this workload "
+                                       "(profiles/plane_staged_kernel_128cubed.md), not "
+                                       "measured in this run",
                      "peak_source": "shared-memory read bandwidth measured in this run "
                                     "(wrt_measure_smem_bandwidth); 32 B per trilinear sample",
                      "hbm": {"achieved": hbm_bytes / per_launch_s / 1e9, "peak": hbm_peak,
@@ -481,6 +836,10 @@ def run_ours(args, dist):
     if plain:
         result["plain"] = plain
         result["served_over_plain"] = e2e_value / plain["value"]
+    if not args.no_other_paths:
+        result["paths"] = other_paths(wrt, ctx, phantom, max(3, min(args.steps, 10)), args.warmup,
+                                      smem_bw, dist.rank == 0 and not args.no_cpu_baseline)
+        result["batch_vs_one_per_launch"] = batch_vs_one_per_launch(wrt, ctx, 3)
     if dist.rank == 0 and dist.world == 1 and not args.no_serving_mix:
         result["serving"] = serving_mix(wrt, dev, args.mix_requests, 4000, 60 << 30)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
@@ -636,13 +995,17 @@ def main():
     ap.add_argument("--kernel", choices=["auto", "plain", "staged"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving-mix", action="store_true")
+    ap.add_argument("--no-other-paths", action="store_true",
+                    help="skip the ray / reduction / adjoint and batching measurements")
     ap.add_argument("--only-kernel", action="store_true",
                     help="time the kernel steps only (for profiling captures)")
     ap.add_argument("--mix-requests", type=int, default=96,
                     help="requests in the mixed serving stream")
     ap.add_argument("--tile", type=int, default=None,
                     help="use this tile configuration of the staged kernel instead of tuning")
-    ap.add_argument("--path", choices=["forward", *PATHS], default="forward",
+    ap.add_argument("--requests", type=int, default=10000,
+                    help="--path serving: requests in the Poisson stream")
+    ap.add_argument("--path", choices=["forward", "serving", *PATHS], default="forward",
                     help="forward: the headline (plane integrals at 128^3); ray, reduction, "
                          "adjoint: the other hot paths through their drop-in entry points")
     ap.add_argument("--grid", default=None,
@@ -653,7 +1016,9 @@ def main():
         NPHI, NTHETA, NSHIFT = (int(x) for x in args.grid.split(","))
     dist = Dist(args.gpus)
     try:
-        if args.path != "forward":
+        if args.path == "serving":
+            rc = serving_stream(args, dist) if args.impl == "ours" and dist.rank == 0 else 0
+        elif args.path != "forward":
             rc = run_path(args, dist) if args.impl == "ours" else 0
         else:
             rc = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)

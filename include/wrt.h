@@ -341,8 +341,9 @@ int wrt_ctx_timer_start(wrt_ctx *ctx);
 int wrt_ctx_timer_stop(wrt_ctx *ctx, float *ms);
 /* Overwrite a device buffer larger than the L2 cache (evicts the volume). */
 int wrt_ctx_flush_l2(wrt_ctx *ctx);
-/* When on, the plane kernels count the lattice samples they evaluate (one
- * atomic per plane).  wrt_ctx_sample_count waits for the stream and returns
+/* When on, the plane and ray kernels count the lattice samples they evaluate
+ * (one atomic per plane or ray) and the reduction kernel the slice samples
+ * (three spline evaluations each).  wrt_ctx_sample_count waits for the stream and returns
  * the running total. */
 int wrt_ctx_count_samples(wrt_ctx *ctx, int on);
 int wrt_ctx_sample_count(wrt_ctx *ctx, uint64_t *count);

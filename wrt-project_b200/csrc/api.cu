@@ -905,6 +905,7 @@ int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const double *f
   job.r2bits = vol->d_stats;
   job.margin = sampler_margin(n, WRT_SAMPLER_TRILINEAR);
   job.out = dev_out;
+  job.counter = ctx->d_counter;
   if (identity) {
     job.pairs = vol->d_pairs;
     job.pitch = vol->pitch;

@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) 
       acc += (double)part;
     }
   }
+  if (job.counter && any) atomicAdd(job.counter, (unsigned long long)(khi - klo + 1));
   job.out[((long long)iz * job.nshift + is) * job.nphi + ip] = acc * delta;
 }
 

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256)
     reduction_kernel(const float4 *__restrict__ lines /* [iz][iphi][ns_ray-1] */, int ngrid,
                      int ns_ray, int nphi, const double *__restrict__ shift, int nshift,
                      const double *__restrict__ cs /* [ntheta][2] cos, sin */, int ntheta,
-                     double *__restrict__ out) {
+                     double *__restrict__ out, unsigned long long *counter) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long total = (long long)nshift * nphi * ntheta;
   if (k >= total) return;
@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(256)
     else kmax = min(half, (int)floor(sqrt(r) / dtau) + 1);
   }
   double acc = 0.0;
+  int evaluated = 0;
   const size_t line_len = (size_t)(ns_ray - 1);
   for (int itau = -kmax; itau <= kmax; ++itau) {
     const double tau = __dmul_rn((double)itau, dtau);
@@ -97,7 +98,9 @@ __global__ void __launch_bounds__(256)
     // quadratic through (z0, v0), (z0+dz, v1), (z0+2dz, v2) at z0 + f dz
     const float val = v0 + f * (v1 - v0) + 0.5f * f * (f - 1.0f) * (v2 - 2.0f * v1 + v0);
     acc += (double)val;
+    ++evaluated;
   }
+  if (counter) atomicAdd(counter, (unsigned long long)evaluated);
   out[k] = acc * dtau;
 }
 
@@ -179,8 +182,8 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
   if (st) return st;
   const long long total = (long long)nshift * nphi * ntheta;
   const long long blocks = (total + 255) / 256;
-  reduction_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(d_lines, ngrid, nshift_ray, nphi,
-                                                              d_shift, nshift, d_cs, ntheta, d_out);
+  reduction_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+      d_lines, ngrid, nshift_ray, nphi, d_shift, nshift, d_cs, ntheta, d_out, ctx->d_counter);
   ctx->launches++;
   return check_launch(ctx, "reduction_kernel");
 }

@@ -276,6 +276,7 @@ struct RayJob {
   double *out;          // [nslices][nshift][nphi]
   const float2 *pairs;  // layer pairs [n-1][n][pitch] of the volume, or null
   int pitch;
+  unsigned long long *counter;  // optional: samples evaluated
 };
 int ray_forward(wrt_ctx *ctx, const RayJob &job);
 
