@@ -42,6 +42,7 @@ struct wrt_grid {
   float *d_shift32 = nullptr; // [nshift]
   double *d_cs = nullptr;     // [ntheta][2]: cos, sin theta (reduction, slicing.c:104-105)
   double4 *d_dirw = nullptr;  // [nphi*ntheta]: omega / h, dphi * w_theta (backprojection)
+  std::vector<double4> dirw;  // host copy of d_dirw
   size_t bytes = 0;
 };
 
@@ -521,7 +522,8 @@ int wrt_grid_create(wrt_ctx *ctx, int nphi, int ntheta, int nshift, wrt_grid **o
   if (!st) st = ctx_alloc(ctx, (void **)&g->d_dir32, sizeof(float) * dir32.size());
   if (!st) st = ctx_alloc(ctx, (void **)&g->d_shift32, sizeof(float) * nshift);
   std::vector<double> cs(2 * (size_t)ntheta);
-  std::vector<double4> dirw(ndir);
+  std::vector<double4> &dirw = g->dirw;
+  dirw.resize(ndir);
   if (!st) {
     for (int i = 0; i < ntheta; ++i) {
       cs[2 * i] = cos(g->theta[i]);  // slicing.c:104-105 evaluate cos/sin(p_theta)
@@ -972,7 +974,7 @@ int wrt_radon3d_adjoint_device(wrt_ctx *ctx, const double *dev_radon, const wrt_
   int st = set_device(ctx);
   if (st) return st;
   return adjoint_forward(ctx, dev_radon, grid->nphi, grid->ntheta, grid->nshift, grid->d_dirw,
-                         ngrid, dev_out);
+                         grid->dirw.data(), ngrid, dev_out);
 }
 
 int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta, int nshift,

@@ -15,13 +15,17 @@
 //   layer pairs of freshly uploaded volumes) -> request prep (crop radius,
 //   fixed-point scale) -> persistent staged plane kernel over the work items
 //   of every forward request, largest first -> finalize (fixed point to FP64)
-//   -> spline prep of every backprojection's lines -> backprojection.
+//   -> spline prep of every backprojection's lines;
+//
+// then, on the same stream, each backprojection's launches (its direction
+// constants are launch parameters, which a graph replayed unchanged cannot
+// carry).
 //
 // Every kernel has a fixed grid and reads its work from the table, which is
 // what lets one captured graph serve batches of any composition.  A request's
 // result is bitwise the same alone or in any batch: the plane sums are
 // order-independent fixed-point integers and the backprojection of a voxel is
-// one thread's sequential sum.
+// one thread's sequential sum, by the same kernel as a single request's.
 #include <string.h>
 
 #include <algorithm>
@@ -157,29 +161,7 @@ __global__ void batch_spline_kernel(const char *t) {
   }
 }
 
-// Backprojection of every voxel of every adjoint request: the voxel-block
-// warps of all requests, taken in turn by the grid's warps.
-__global__ void __launch_bounds__(256, 2) batch_adjoint_kernel(const char *t) {
-  const int na = hdr(t)->nadj;
-  const AdjReq *J = adj_tab(t);
-  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
-  const long long nw = (long long)gridDim.x * blockDim.x / 32;
-  const int lane = threadIdx.x & 31;
-  long long first = 0;  // global index of request r's first warp
-  for (int r = 0; r < na; ++r) {
-    const int n = J[r].n;
-    const long long warps = wrtd::adjoint_warps(n);
-    // warps continue from one request to the next so that small requests do
-    // not leave most of the grid idle
-    long long w = gw - first % nw;
-    if (w < 0) w += nw;
-    for (; w < warps; w += nw)
-      wrtd::adjoint_block(J[r].lines, J[r].ndir, J[r].nshift, J[r].dirw, n, w, lane, J[r].out);
-    first += warps;
-  }
-}
-
-constexpr int kBatchKernels = 7;  // kernels per graph launch
+constexpr int kBatchKernels = 6;  // kernels per graph launch
 
 }  // namespace
 
@@ -285,7 +267,6 @@ int capture(BatchSlot *s) {
   if (!st) {
     batch_finalize_kernel<<<g, 256, 0, s->stream>>>(s->d_table);
     batch_spline_kernel<<<g, 128, 0, s->stream>>>(s->d_table);
-    batch_adjoint_kernel<<<g, 256, 0, s->stream>>>(s->d_table);
     e = cudaGetLastError();
     if (e != cudaSuccess) st = cuda_fail(ctx, e, "batch kernels");
   }
@@ -359,6 +340,12 @@ int batch_slot_launch(BatchSlot *s, BatchBuilder &b) {
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch event");
   s->launched = true;
   ctx->launches += kBatchKernels;
+  // the backprojections, behind the graph (which built their spline lines):
+  // their direction constants travel as launch parameters
+  for (const AdjReq &j : b.adj) {
+    e = launch_adjoint(s->stream, j.lines, j.ndir, j.nshift, j.h_dirw, j.n, j.out, &ctx->launches);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch adjoint_kernel");
+  }
   return WRT_OK;
 }
 

@@ -33,8 +33,6 @@ namespace wrt {
 cudaError_t launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int ndir, int nshift,
                                  const double *d_cp, const double *d_den, double *d_scratch,
                                  float4 *d_lines, const double4 *d_dirw);
-cudaError_t launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int nshift,
-                           const double4 *d_dirw, int n, double *d_out);
 }  // namespace wrt
 
 namespace {
@@ -140,8 +138,8 @@ extern "C" int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, i
   e = wrt::launch_adjoint_lines(s, d_radon, (int)ndir, nshift, cp, den, M, lines, dirw);
   if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "radon3d_adjoint_static: spline_prep_kernel");
   ctx->launches++;
-  e = wrt::launch_adjoint(s, lines, (int)ndir, nshift, dirw, ngrid, d_out);
+  e = wrt::launch_adjoint(s, lines, (int)ndir, nshift, h_dirw.data(), ngrid, d_out,
+                          &ctx->launches);
   if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "radon3d_adjoint_static: adjoint_kernel");
-  ctx->launches++;
   return WRT_OK;
 }

@@ -105,17 +105,16 @@ __global__ void __launch_bounds__(256)
 }
 
 // Adjoint: one warp per voxel block of wrtd::adjoint_block (8 x 4 columns of
-// V voxels), output order [iz][ix][iy]; every lane loops over all directions.
-// dirw[d] = (omega / h, dphi * w_theta).
-__global__ void __launch_bounds__(256, 3)
-    adjoint_kernel(const float4 *__restrict__ lines /* [d][ns-1] */, int ndir, int ns,
-                   const double4 *__restrict__ dirw, int n, double *__restrict__ out) {
+// V voxels), output order [iz][ix][iy]; one launch per kAdjDirsPerLaunch
+// directions, their constants in the parameter space.
+template <int V>
+__global__ void __launch_bounds__(256, V == 4 ? 3 : 2)
+    adjoint_kernel(const float4 *__restrict__ lines /* [d][ns-1] */, int ns, int dbeg, int nd,
+                   const __grid_constant__ wrtd::AdjDirs dirs, int n, double *__restrict__ out) {
   const long long w = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   if (w >= wrtd::adjoint_warps(n)) return;
-  wrtd::adjoint_block(lines, ndir, ns, dirw, n, w, threadIdx.x & 31, out);
+  wrtd::adjoint_block<V>(lines, ns, dbeg, nd, dirs, n, w, threadIdx.x & 31, out);
 }
-
-unsigned adjoint_blocks(int n) { return (unsigned)((wrtd::adjoint_warps(n) + 7) / 8); }
 
 // Natural splines of nlines lines into the context's workspace (records in
 // WS_LINES); asynchronous on the context's stream.
@@ -167,9 +166,29 @@ cudaError_t launch_adjoint_lines(cudaStream_t stream, const double *d_radon, int
 }
 
 cudaError_t launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int nshift,
-                           const double4 *d_dirw, int n, double *d_out) {
-  adjoint_kernel<<<adjoint_blocks(n), 256, 0, stream>>>(d_lines, ndir, nshift, d_dirw, n, d_out);
-  return cudaGetLastError();
+                           const double4 *h_dirw, int n, double *d_out, uint64_t *launches) {
+  // parameters of one launch, filled on the host (the launch copies them)
+  static thread_local wrtd::AdjDirs dirs;
+  const int V = wrtd::adjoint_vox(n);
+  const unsigned blocks = (unsigned)((wrtd::adjoint_warps(n) + 7) / 8);
+  for (int d0 = 0; d0 < ndir; d0 += wrtd::kAdjDirsPerLaunch) {
+    const int nd = ndir - d0 < wrtd::kAdjDirsPerLaunch ? ndir - d0 : wrtd::kAdjDirsPerLaunch;
+    for (int j = 0; j < nd; ++j) {
+      const double4 g = h_dirw[d0 + j];
+      dirs.g[j][0] = g.x;
+      dirs.g[j][1] = g.y;
+      dirs.g[j][2] = g.z;
+      wrtd::adjoint_header(g.x, n, nshift, V, &dirs.hd[j]);
+    }
+    if (V == 8)
+      adjoint_kernel<8><<<blocks, 256, 0, stream>>>(d_lines, nshift, d0, nd, dirs, n, d_out);
+    else
+      adjoint_kernel<4><<<blocks, 256, 0, stream>>>(d_lines, nshift, d0, nd, dirs, n, d_out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (launches) ++*launches;
+  }
+  return cudaSuccess;
 }
 
 int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_ray, int nphi,
@@ -189,16 +208,15 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
 }
 
 int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
-                    const double4 *d_dirw, int n, double *d_out) {
+                    const double4 *d_dirw, const double4 *h_dirw, int n, double *d_out) {
   // lines (iphi, itheta): element is at d_radon[(is*nphi + iphi)*ntheta + itheta]
   float4 *d_lines = nullptr;
   const int ndir = nphi * ntheta;
   int st = prep_lines(ctx, d_radon, ndir, ndir, 0, (long long)ndir, 1, nshift, &d_lines, d_dirw);
   if (st) return st;
-  adjoint_kernel<<<adjoint_blocks(n), 256, 0, ctx->stream>>>(d_lines, ndir, nshift, d_dirw, n,
-                                                              d_out);
-  ctx->launches++;
-  return check_launch(ctx, "adjoint_kernel");
+  cudaError_t e = launch_adjoint(ctx->stream, d_lines, ndir, nshift, h_dirw, n, d_out,
+                                 &ctx->launches);
+  return e == cudaSuccess ? WRT_OK : cuda_fail(ctx, e, "adjoint_kernel");
 }
 
 }  // namespace wrt

@@ -54,6 +54,7 @@ struct GridTables {
   double *shift = nullptr;   // [nshift]
   float *shift32 = nullptr;  // [nshift]
   double4 *dirw = nullptr;   // [ndir]
+  std::vector<double4> h_dirw;  // host copy (backprojection launch parameters)
   double *cp = nullptr, *den = nullptr;  // [nshift]
   int nphi = 0, ntheta = 0, nshift = 0;
   int refs = 0;
@@ -149,7 +150,8 @@ int make_grid(wrt_server *s, GridTables &g) {
   for (int i = 0; i < nshift; ++i) shift32[i] = (float)shift[i];
   // backprojection weights (backprojection/C/src/integral.c:11-18) and the
   // natural-spline elimination coefficients
-  std::vector<double4> dirw(ndir);
+  std::vector<double4> &dirw = g.h_dirw;
+  dirw.resize(ndir);
   wrt::adjoint_directions(nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), dirw.data());
   std::vector<double> cp(nshift, 0.0), den(nshift, 1.0);
   for (int i = 1; i + 1 < nshift; ++i) {
@@ -321,6 +323,7 @@ void add_to_batch(wrt_server *s, Request *q, wrt::BatchBuilder &b) {
     j.lines = reinterpret_cast<float4 *>(base + al(8 * nplanes) + al(8 * (size_t)ndir * r.nshift));
     j.out = q->d_out;
     j.dirw = g->dirw;
+    j.h_dirw = g->h_dirw.data();
     j.cp = g->cp;
     j.den = g->den;
     j.ndir = ndir;

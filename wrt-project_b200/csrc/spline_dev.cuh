@@ -15,6 +15,8 @@
 //     coefficients formed in FP64 and rounded once.
 #pragma once
 #include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
 
 namespace wrtd {
 
@@ -91,38 +93,49 @@ __device__ __forceinline__ float cubic_centred(const float4 c, float u) {
 // [iz][ix][iy] at cell centres (radon3d_ajoint.c:240-254):
 //   R*g(x) = sum over directions d of dphi*w_theta * S_d(<x, omega_d>),
 //   S_d = 0 beyond |s| > 1.
-// The direction table holds g_d = (omega_d / h, dphi * w_theta) in FP64
-// (h = 2/(ns-1)), so a voxel's knot position is q = <x, g_d> + 1/h and the
-// interval record of knot floor(q) gives the value (the weight is folded into
-// the adjoint lines).
+// With g_d = omega_d / h (h = 2/(ns-1)) a voxel's knot position is
+// q = <x, g_d> + 1/h, and the interval record of knot floor(q) gives the
+// value (the direction's weight is folded into its adjoint line).
+//
+// Direction constants reach the kernel through its parameter space (the
+// constant bank, read once per warp) in launches of kAdjDirsPerLaunch
+// directions: per direction g_d in FP64 and a header for the volume's edge n,
+// so the L1 data path carries only the spline records.  The voxel sums are
+// carried from launch to launch in the output buffer (FP64).
 //
 // Work split: a warp owns a block of 8 (y) x 4 (z) voxel columns and V
 // consecutive voxels along x in each (lane = one column, V voxels).  For one
 // direction the 32 columns' knot positions lie within (7 |g_y| + 3 |g_z|) * 2/n
 // knots of each other, so the warp's loads touch two or three 128-byte lines
-// of the direction's spline; the V voxels of a lane step q by dq = (2/n) g_x.
+// of the direction's spline.
 //
-// Per (lane, direction), in FP64: q0 = q - 1/2 of the lane's first voxel,
-// split exactly into the integer i0 = rint(q0) and the FP32 remainder f0 in
-// [-1/2, 1/2] (the 1.5 * 2^52 rounding constant), the same split of the
-// per-voxel step dq = di + df, and the range of the V positions.  When all of
-// them lie at least kAdjGuard knots inside [0, ns-1] (|s| < 1 with margin),
-// each voxel costs FP32 work only: f = f0 + v df (|f| <= 2), k = rint(f) and
-// u = f - k by the 1.5 * 2^23 rounding constant, the record at knot
-// i0 + v di + k (in [0, ns-2] by the margin), and a Horner cubic in u.  The
-// FP32 error of f is below 3e-7 knots.  A lane whose positions come within
-// the guard band of |s| = 1, where S_d jumps to zero, evaluates that
-// direction in FP64 per voxel with the exact range test; a lane entirely
-// outside skips it.  Values are summed in FP32 over chunks of kAdjChunk
-// directions and the chunk sums in FP64, in a fixed order: a voxel's result
-// does not depend on how requests are batched.
+// Per (lane, direction), in FP64: q0 = q - 1/2 of the lane's first voxel and
+// its exact split into the integer i0 = rint(q0) and the FP32 remainder f0 in
+// [-1/2, 1/2] (1.5 * 2^52 rounding constant).  The per-voxel step
+// dq = (2/n) g_x is split the same way on the host, dq = di + df.  Voxel v
+// then has q - 1/2 = i0 + v di + f_v, f_v = f0 + v df, |f_v| <= V/2.  When
+// i0 lies in the header's window [lo, lo + span] every one of the V positions
+// is at least one knot inside [0, ns-1] (|s| < 1), and each voxel costs FP32
+// work only, two voxels per packed f32x2 instruction: f_v, k = rint(f_v) and
+// u = f_v - k by the 1.5 * 2^23 rounding constant, the record at knot
+// i0 + v di + k (in [1, ns-3] by the window), a Horner cubic in u.  The FP32
+// error of f_v is below 3e-7 knots.  Other lanes test the range exactly per
+// voxel in FP64 (where S_d jumps to zero at |s| = 1), or skip the direction
+// when the window shows every position outside.  Values are summed in FP32
+// over chunks of kAdjChunk directions and the chunk sums in FP64, in a fixed
+// order: a voxel's result does not depend on how requests are batched.
 constexpr int kAdjLanesY = 8, kAdjLanesZ = 4;
 constexpr int kAdjChunk = 32;
-constexpr double kAdjGuard = 1e-4;
+constexpr int kAdjDirsPerLaunch = 768;  // a multiple of kAdjChunk
 
-// voxels per lane along x (4: 80 registers, three 256-thread blocks per SM;
-// 8 voxels need 110 registers and halve the resident warps)
-__host__ __device__ inline int adjoint_vox(int) { return 4; }
+struct AdjDirs {             // one launch's direction constants (30 KB of parameters)
+  double g[kAdjDirsPerLaunch][3];  // omega / h
+  int4 hd[kAdjDirsPerLaunch];      // float bits of df, di, lo, span
+};
+
+// voxels per lane along x: 8 from edge 192 up (fewer direction set-ups per
+// evaluation), 4 below (more warps for smaller volumes)
+__host__ __device__ inline int adjoint_vox(int n) { return n >= 192 ? 8 : 4; }
 
 __host__ __device__ inline long long adjoint_warps(int n) {
   const int V = adjoint_vox(n);
@@ -130,11 +143,57 @@ __host__ __device__ inline long long adjoint_warps(int n) {
          ((n + V - 1) / V);
 }
 
+// Header of direction g (x component gx) for edge n, ns shifts, V voxels:
+// df, di, and the window [lo, lo + span] of i0 for which every position
+// q_v - 1/2 = i0 + v di + f_v (|f_v| <= V/2) satisfies 1 <= q_v <= ns - 2.
+inline void adjoint_header(double gx, int n, int ns, int V, int4 *hd) {
+  const double dq = (2.0 / n) * gx;
+  const double ts = dq + 6755399441055744.0;
+  const long long di = llrint(ts - 6755399441055744.0);
+  const float df = (float)(dq - (ts - 6755399441055744.0));
+  const long long mn = di < 0 ? (V - 1) * di : 0, mx = di > 0 ? (V - 1) * di : 0;
+  long long lo = V / 2 + 1 - mn, hi = (long long)ns - 3 - V / 2 - mx;
+  int span = (int)(hi - lo);
+  if (hi < lo) {  // no lane can take the FP32 path for this direction
+    lo = 0x40000000;
+    span = 0;
+  }
+  int dfb;
+  memcpy(&dfb, &df, sizeof(dfb));
+  *hd = make_int4(dfb, (int)di, (int)lo, span);
+}
+
+typedef unsigned long long adj_u64;
+__device__ __forceinline__ adj_u64 adj_pk(float lo, float hi) {
+  adj_u64 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void adj_upk(adj_u64 r, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(r));
+}
+__device__ __forceinline__ adj_u64 adj_fma2(adj_u64 a, adj_u64 b, adj_u64 c) {
+  adj_u64 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ adj_u64 adj_add2(adj_u64 a, adj_u64 b) {
+  adj_u64 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ adj_u64 adj_sub2(adj_u64 a, adj_u64 b) {
+  adj_u64 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// Warp w (0 <= w < adjoint_warps(n)) over directions [dbeg, dbeg + nd) of an
+// n^3 backprojection; lines[d] holds direction d's ns-1 records.
 template <int V>
-__device__ __forceinline__ void adjoint_block_v(const float4 *__restrict__ lines, int ndir, int ns,
-                                                const double4 *__restrict__ dirw, int n,
-                                                long long w, int lane,
-                                                double *__restrict__ out) {
+__device__ __forceinline__ void adjoint_block(const float4 *__restrict__ lines, int ns, int dbeg,
+                                              int nd, const AdjDirs &dirs, int n, long long w,
+                                              int lane, double *__restrict__ out) {
   const int nby = (n + kAdjLanesY - 1) / kAdjLanesY, nbz = (n + kAdjLanesZ - 1) / kAdjLanesZ;
   const int by = (int)(w % nby);
   const long long r = w / nby;
@@ -150,51 +209,57 @@ __device__ __forceinline__ void adjoint_block_v(const float4 *__restrict__ lines
   const double qoff = 0.5 * (double)(ns - 1) - 0.5;  // 1/h - 1/2
   const double qmax = (double)(ns - 1);
   const double dx = 2.0 / n;
-  const double fast_lo = kAdjGuard - 0.5, fast_hi = qmax - 0.5 - kAdjGuard;
-  const double out_lo = -0.5 - kAdjGuard, out_hi = qmax - 0.5 + kAdjGuard;
   const size_t line_len = (size_t)(ns - 1);
+  const size_t o = ((size_t)iz * n + ix0) * n + iy;
   double tot[V];
 #pragma unroll
-  for (int v = 0; v < V; ++v) tot[v] = 0.0;
-  for (int d0 = 0; d0 < ndir; d0 += kAdjChunk) {
-    const int d1 = min(ndir, d0 + kAdjChunk);
+  for (int v = 0; v < V; ++v) tot[v] = (dbeg == 0 || ix0 + v >= n) ? 0.0 : out[o + (size_t)v * n];
+  const adj_u64 MM = adj_pk(12582912.0f, 12582912.0f);  // 1.5 * 2^23
+  for (int j0 = 0; j0 < nd; j0 += kAdjChunk) {
+    const int j1 = min(nd, j0 + kAdjChunk);
     float acc[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = 0.0f;
-#pragma unroll 2
-    for (int d = d0; d < d1; ++d) {
-      const double2 gxy = __ldg(reinterpret_cast<const double2 *>(dirw + d));
-      const double gz = __ldg(reinterpret_cast<const double *>(dirw + d) + 2);
-      const double q0 = fma(x0, gxy.x, fma(y, gxy.y, fma(z, gz, qoff)));
-      const double dq = dx * gxy.x;
-      const double qe = fma((double)(V - 1), dq, q0);
-      const double lo = fmin(q0, qe), hi = fmax(q0, qe);
-      const float4 *line = lines + (size_t)d * line_len;
-      if (lo > fast_lo && hi < fast_hi) {
-        const double t64 = q0 + 6755399441055744.0;  // 1.5 * 2^52
-        const int i0 = __double2loint(t64);           // rint(q0)
+#pragma unroll 1
+    for (int j = j0; j < j1; ++j) {
+      const float4 *line = lines + (size_t)(dbeg + j) * line_len;
+      const int4 hd = dirs.hd[j];
+      const double q0 = fma(x0, dirs.g[j][0], fma(y, dirs.g[j][1], fma(z, dirs.g[j][2], qoff)));
+      const double t64 = q0 + 6755399441055744.0;  // 1.5 * 2^52
+      const int i0 = __double2loint(t64);           // rint(q0)
+      if ((unsigned)(i0 - hd.z) <= (unsigned)hd.w) {
         const float f0 = (float)(q0 - (t64 - 6755399441055744.0));
-        const double ts = dq + 6755399441055744.0;
-        const int di = __double2loint(ts);            // rint(dq)
-        const float dqf = (float)(dq - (ts - 6755399441055744.0));
+        const float df = __int_as_float(hd.x);
+        const int di = hd.y;
         const float4 *base = line + (i0 - 0x4B400000);
+        const adj_u64 F0 = adj_pk(f0, f0), DF = adj_pk(df, df);
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          // q - 1/2 = i0 + v di + f, |f| <= 1/2 + v/2
-          const float f = fmaf((float)v, dqf, f0);
-          const float t = f + 12582912.0f;  // 1.5 * 2^23: rint(f) in the low bits
-          const float u = f - (t - 12582912.0f);
-          const float4 c = __ldg(base + (__float_as_int(t) + v * di));
-          acc[v] += cubic_centred(c, u);
+        for (int v = 0; v < V; v += 2) {
+          const adj_u64 f = adj_fma2(adj_pk((float)v, (float)(v + 1)), DF, F0);
+          const adj_u64 t = adj_add2(f, MM);
+          const adj_u64 u = adj_sub2(f, adj_sub2(t, MM));
+          float ta, tb, ua, ub;
+          adj_upk(t, ta, tb);
+          adj_upk(u, ua, ub);
+          const float4 ca = __ldg(base + (__float_as_int(ta) + v * di));
+          const float4 cb = __ldg(base + (__float_as_int(tb) + (v + 1) * di));
+          acc[v] += cubic_centred(ca, ua);
+          acc[v + 1] += cubic_centred(cb, ub);
         }
-      } else if (hi >= out_lo && lo <= out_hi) {
+      } else {
+        const int di = hd.y;
+        const int mn = min(0, (V - 1) * di), mx = max(0, (V - 1) * di);
+        // every position certainly outside [0, ns-1]: nothing to add
+        if (!(i0 + mx <= -V / 2 - 1 || i0 + mn >= ns + V / 2 - 1)) {
+          const double dq = dx * dirs.g[j][0];
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-          const double q = fma((double)v, dq, q0) + 0.5;
-          if (q >= 0.0 && q <= qmax) {  // |s| <= 1 (interp.c:9-11)
-            const int i = min(__double2int_rz(q), ns - 2);
-            const float u = (float)((q - (double)i) - 0.5);
-            acc[v] += cubic_centred(__ldg(line + i), u);
+          for (int v = 0; v < V; ++v) {
+            const double q = fma((double)v, dq, q0) + 0.5;
+            if (q >= 0.0 && q <= qmax) {  // |s| <= 1 (interp.c:9-11)
+              const int i = min(__double2int_rz(q), ns - 2);
+              const float u = (float)((q - (double)i) - 0.5);
+              acc[v] += cubic_centred(__ldg(line + i), u);
+            }
           }
         }
       }
@@ -202,17 +267,9 @@ __device__ __forceinline__ void adjoint_block_v(const float4 *__restrict__ lines
 #pragma unroll
     for (int v = 0; v < V; ++v) tot[v] += (double)acc[v];
   }
-  const size_t o = ((size_t)iz * n + ix0) * n + iy;
 #pragma unroll
   for (int v = 0; v < V; ++v)
     if (ix0 + v < n) out[o + (size_t)v * n] = tot[v];
-}
-
-// Warp w (0 <= w < adjoint_warps(n)) of an n^3 backprojection.
-__device__ __forceinline__ void adjoint_block(const float4 *__restrict__ lines, int ndir, int ns,
-                                              const double4 *__restrict__ dirw, int n,
-                                              long long w, int lane, double *__restrict__ out) {
-  adjoint_block_v<4>(lines, ndir, ns, dirw, n, w, lane, out);
 }
 
 }  // namespace wrtd

@@ -208,6 +208,7 @@ struct AdjReq {                    // one backprojection
   double *scratch;                 // [ndir][nshift]
   float4 *lines;                   // [ndir][nshift - 1]
   double *out;                     // [iz][ix][iy]
+  const double4 *h_dirw;           // host copy of dirw (launch parameters)
   int ndir, ntheta, nshift, n;
 };
 struct BatchHeader {
@@ -292,9 +293,14 @@ int reduction_forward(wrt_ctx *ctx, const double *d_rays, int ngrid, int nshift_
                       int nphi, const double *d_shift, int nshift,
                       const double *d_cs /* [ntheta][2]: cos, sin theta */, int ntheta,
                       double *d_out);
+// d_dirw / h_dirw: the same direction table [nphi*ntheta] (omega/h, dphi*w) on
+// the device (spline weights) and on the host (per-launch constants).
 int adjoint_forward(wrt_ctx *ctx, const double *d_radon, int nphi, int ntheta, int nshift,
-                    const double4 *d_dirw /* [nphi*ntheta]: omega/h, dphi*w */, int n,
-                    double *d_out);
+                    const double4 *d_dirw, const double4 *h_dirw, int n, double *d_out);
+// The backprojection launches over prepared adjoint lines [ndir][nshift-1] on a
+// stream (one launch per kAdjDirsPerLaunch directions; *launches counts them).
+cudaError_t launch_adjoint(cudaStream_t stream, const float4 *d_lines, int ndir, int nshift,
+                           const double4 *h_dirw, int n, double *d_out, uint64_t *launches);
 
 }  // namespace wrt
 
