@@ -2,13 +2,19 @@
 checked against the FP64 oracle on seeded random subsets (the oracle at these
 sizes would take hours in full):
 
+* the CPU configuration on the GPU at its own grid: 64^3, 32 x 64 sphere grid
+  x 128 shifts, 128^2 trilinear lattice, and the reference's default nearest
+  sampler on its 4n x 4n lattice, 4,096 seeded planes each;
+
 * ray transform + reduction at 128^3: 64 layer orientations x 128 layers x
-  128 ray angles x 128 ray offsets; ray data reduced to a 64 x 128 sphere grid
-  with 256 shifts (decoupled from the 128 ray offsets);
+  128 ray angles x 128 ray offsets (24 seeded rays of every orientation against
+  the oracle); ray data reduced to a 64 x 128 sphere grid with 256 shifts
+  (decoupled from the 128 ray offsets);
 * 64 volumes of uneven edge lengths, each with its own sphere grid and shift
   count, in ONE batched launch; relative error per volume;
-* 256^3 in FP32 and BF16 storage on a 96 x 192 sphere grid with 384 shifts;
-  the backprojection back to 256^3 of seeded Gaussian Radon data; and the
+* 256^3 in FP32 and BF16 storage on a 96 x 192 sphere grid with 384 shifts
+  (4,096 seeded planes each); the backprojection back to 256^3 of seeded
+  Gaussian Radon data (a 32^3 voxel block and 256 scattered voxels); and the
   inner-product test <R f, g> = <f, R^T g> with the exact transpose.
 
 Each volume is a sum of seeded ellipsoids (centres in the ball of radius 0.6,
@@ -32,6 +38,20 @@ def _planes_subset(rng, nphi, ntheta, nshift, count):
     return (i_s, ip, it), (phi[ip], theta[it], shift[i_s])
 
 
+@pytest.mark.parametrize("sampler", [O.TRILINEAR, O.NEAREST])
+def test_cpu_configuration_64_cubed_at_its_grid(ctx, sampler):
+    n, nphi, ntheta, nshift = 64, 64, 32, 128
+    vol = ellipsoid_phantom(n, 8, 1000)
+    L = n if sampler == O.TRILINEAR else 2 * n  # 128^2 trilinear; reference 4n x 4n nearest
+    got = ctx.radon_grid(vol, nphi, ntheta, nshift, sampler=sampler, half_extent=L)
+    rng = np.random.default_rng(64 + sampler)
+    (i_s, ip, it), (p, t, s) = _planes_subset(rng, nphi, ntheta, nshift, 4096)
+    ref = O.radon_planes(vol, p, t, s, sampler=sampler, half_extent=L)
+    err = rel_l2(got[i_s, ip, it], ref)
+    print(f"64^3 {'trilinear' if sampler else 'nearest'}: rel. L2 {err:.2e} on 4096 planes")
+    assert err < TOL_L2
+
+
 def test_rays_64_orientations_and_decoupled_reduction_128(ctx):
     n = 128
     vol = ellipsoid_phantom(n, 16, 1001)
@@ -41,20 +61,20 @@ def test_rays_64_orientations_and_decoupled_reduction_128(ctx):
     errs = []
     for k, F in enumerate(frames):
         rays = ctx.ray_grid(vol, n, 128, 128, frame=None if k == 0 else F)
-        if k % 8 == 0:  # oracle on 24 random rays of every 8th orientation
-            iz, i_s, ip = (rng.integers(0, 128, 24) for _ in range(3))
-            got = rays[iz, i_s, ip]
-            ref = np.array([O.ray_transform(vol, -1.0 + 2.0 * a / (n - 1), shifts[b], phis[c],
-                                            frame=None if k == 0 else F)
-                            for a, b, c in zip(iz, i_s, ip)])
-            errs.append(rel_l2(got, ref))
+        # oracle on 24 seeded rays of every orientation
+        iz, i_s, ip = (rng.integers(0, 128, 24) for _ in range(3))
+        got = rays[iz, i_s, ip]
+        ref = np.array([O.ray_transform(vol, -1.0 + 2.0 * a / (n - 1), shifts[b], phis[c],
+                                        frame=None if k == 0 else F)
+                        for a, b, c in zip(iz, i_s, ip)])
+        errs.append(rel_l2(got, ref))
         if k == 0:
             rays0 = rays
     assert max(errs) < TOL_L2, errs
     # reduction of orientation 0's rays (128 offsets) to 256 Radon shifts
     radon = ctx.radon_reduction(rays0, 256, 64)
     assert radon.shape == (256, 128, 64)
-    sel = rng.integers(0, [256, 128, 64], size=(64, 3))
+    sel = rng.integers(0, [256, 128, 64], size=(1024, 3))
     ref = O.reduction_planes(rays0, 256, 64, sel[:, 0], sel[:, 1], sel[:, 2])
     assert rel_l2(radon[sel[:, 0], sel[:, 1], sel[:, 2]], ref) < TOL_L2
 
@@ -104,7 +124,7 @@ def test_256_cubed_fp32_and_bf16(ctx, vol256, storage):
     wrt.radon_forward_batch(ctx, [(v, g, out.ptr, n)])
     res = out.download(np.empty((nshift, nphi, ntheta)))
     rng = np.random.default_rng(31 + storage)
-    (i_s, ip, it), (p, t, s) = _planes_subset(rng, nphi, ntheta, nshift, 16)
+    (i_s, ip, it), (p, t, s) = _planes_subset(rng, nphi, ntheta, nshift, 4096)
     got = res[i_s, ip, it]
     if storage == wrt.STORAGE_BF16:
         held = O.radon_planes(wrt.round_bf16(vol256), p, t, s, sampler=O.TRILINEAR, half_extent=n)
@@ -125,10 +145,18 @@ def test_256_cubed_backprojection_and_inner_product(ctx, vol256):
     # the reference's backprojection of seeded Gaussian Radon data, back to 256^3
     g = rng.standard_normal((nshift, nphi, ntheta))
     adj = ctx.radon3d_adjoint(g, n)  # [iz][ix][iy], cell centres
-    iz, ix, iy = (rng.integers(0, n, 32) for _ in range(3))
     c = lambda i: -1.0 + 1.0 / n + i * (2.0 / n)
+    # a 32^3 block of voxels at a seeded corner, and 256 voxels anywhere
+    z0, x0, y0 = rng.integers(0, n - 32, 3)
+    bz, bx, by = np.meshgrid(np.arange(z0, z0 + 32), np.arange(x0, x0 + 32),
+                             np.arange(y0, y0 + 32), indexing="ij")
+    iz = np.concatenate([bz.ravel(), rng.integers(0, n, 256)])
+    ix = np.concatenate([bx.ravel(), rng.integers(0, n, 256)])
+    iy = np.concatenate([by.ravel(), rng.integers(0, n, 256)])
     ref = O.adjoint_points(g, c(ix), c(iy), c(iz))
-    assert rel_l2(adj[iz, ix, iy], ref) < TOL_L2
+    err = rel_l2(adj[iz, ix, iy], ref)
+    print(f"256^3 backprojection: rel. L2 {err:.2e} on a 32^3 block + 256 voxels")
+    assert err < TOL_L2
     # inner-product test of the forward transform against its exact transpose:
     # g seeded Gaussian on 2048 random planes (zero elsewhere)
     gs = np.zeros((nshift, nphi, ntheta))
