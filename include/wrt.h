@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define WRT_ABI_VERSION 1
+#define WRT_ABI_VERSION 2
 
 typedef enum wrt_status {
   WRT_OK = 0,
@@ -278,18 +278,28 @@ typedef struct wrt_server wrt_server;
 
 typedef enum wrt_op {
   WRT_OP_FORWARD = 0, /* plane integrals, trilinear sampler (radon_grid/src/integral.c:26) */
-  WRT_OP_ADJOINT = 1  /* backprojection (radon_inversion/backprojection/C/src/integral.c:6) */
+  WRT_OP_ADJOINT = 1, /* backprojection (radon_inversion/backprojection/C/src/integral.c:6) */
+  WRT_OP_RAY = 2,     /* layer-by-layer ray integrals (ray_grid/src/integral.c:11) */
+  WRT_OP_REDUCE = 3   /* ray data to Radon data (radon_reduction/slicing.c:80) */
 } wrt_op;
 
 typedef struct wrt_request {
   int op;              /* wrt_op */
-  int ngrid;           /* n: edge of the input (forward) or output (adjoint) volume */
-  int nphi, ntheta, nshift;
+  int ngrid;           /* n: edge of the input (forward, ray) or output (adjoint) volume;
+                          reduce: z-slices of the ray data */
+  int nphi, ntheta, nshift; /* sphere grid (forward, adjoint, reduce); ray: nphi angles and
+                               nshift offsets per layer (ntheta unused) */
   int half_extent;     /* forward: lattice [-L, L)^2 with step 1/n; 0 means L = 2n */
-  const float *volume; /* forward input: n^3 FP32 values, v[ix][iy][iz] */
+  const float *volume; /* forward and ray input: n^3 FP32 values, v[ix][iy][iz] */
   const double *radon; /* adjoint input: nshift*nphi*ntheta values, [is][iphi][itheta] */
-  double *out;         /* result: forward [is][iphi][itheta]; adjoint [iz][ix][iy] */
+  double *out;         /* result: forward and reduce [is][iphi][itheta]; adjoint
+                          [iz][ix][iy]; ray [iz][is][iphi] */
   uint64_t tag;        /* the caller's, returned in wrt_request_info */
+  int nslices;         /* ray: layers (z-slices) */
+  int nshift_ray;      /* reduce: offsets per ray line of the input */
+  const double *rays;  /* reduce input: ngrid*nshift_ray*nphi values, [iz][is][iphi] */
+  const double *frame; /* ray: NULL (the reference's z-slices) or a row-major 3x3 rotation of
+                          the sample points, read at submission */
 } wrt_request;
 
 typedef struct wrt_request_info {
@@ -301,7 +311,8 @@ typedef struct wrt_request_info {
 
 typedef struct wrt_server_opts {
   int device;          /* CUDA ordinal */
-  int max_batch;       /* requests per launch (0: 64; at most 256 forward + 256 adjoint) */
+  int max_batch;       /* requests per launch (0: 64; at most 256 forward + 256 adjoint
+                          + 64 ray + 64 reduce) */
   int max_inflight;    /* launches on the device at once (0: 2; at most 8) */
   int queue_capacity;  /* requests waiting for admission (0: 65536) */
   size_t hbm_budget;   /* device memory for request state and grid tables

@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = wrt.lib()
-    assert lib.wrt_abi_version() == 1
+    assert lib.wrt_abi_version() == 2
     for code in range(0, 11):
         assert lib.wrt_status_string(code)
     assert lib.wrt_status_string(999) == b"unknown status"

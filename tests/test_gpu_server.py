@@ -167,3 +167,42 @@ def test_requests_arriving_during_a_launch_overlap_it():
     # the later requests were admitted and launched before the first one finished
     assert min(i.start_ms for i in infos) < i0.done_ms
     assert max(i.batch_size for i in infos) > 1
+
+
+def test_served_ray_and_reduction_equal_direct_alone_and_in_the_mix(ctx):
+    """The ray transform and the ray-to-Radon reduction as served requests
+    (WRT_OP_RAY, WRT_OP_REDUCE): bitwise the direct entry points' results, in
+    a batch of their own and among concurrent forward / adjoint requests; and
+    the ray_grid -> radon_reduction chain within the FP32 tolerance of the
+    oracle."""
+    n, nsr, nphi, nshift, ntheta = 24, 20, 12, 16, 6
+    vol = ellipsoid_phantom(n, 6, 808).astype(np.float32)
+    frame = np.array([[0.36, 0.48, -0.8], [-0.8, 0.6, 0.0], [0.48, 0.64, 0.6]])
+    rays_direct = ctx.ray_grid(vol.astype(np.float64), n, nsr, nphi)
+    rays_frame = ctx.ray_grid(vol.astype(np.float64), n, nsr, nphi, frame=frame)
+    radon_direct = ctx.radon_reduction(rays_direct, nshift, ntheta)
+    assert rel_l2(rays_direct, O.ray_forward(vol.astype(np.float64), n, nsr, nphi)) < TOL_L2
+    assert rel_l2(radon_direct, O.reduction_forward(rays_direct, nshift, ntheta)) < TOL_L2
+    rng = np.random.default_rng(77)
+    with wrt.Server(0, budget_bytes=1 << 30, max_batch=16, max_inflight=2) as srv:
+        def three():
+            r0, r1, r2 = (np.zeros((n, nsr, nphi)), np.zeros((n, nsr, nphi)),
+                          np.zeros((nshift, nphi, ntheta)))
+            ids = [srv.submit_ray(vol, n, nsr, nphi, r0),
+                   srv.submit_ray(vol, n, nsr, nphi, r1, frame=frame),
+                   srv.submit_reduce(rays_direct, nshift, ntheta, r2)]
+            return ids, (r0, r1, r2)
+        ids, outs = three()
+        for i in ids:
+            assert srv.wait(i, WAIT_MS).status == 0
+        for got, ref in zip(outs, (rays_direct, rays_frame, radon_direct)):
+            assert np.array_equal(got, ref)
+        # again, among 30 forward / adjoint requests submitted at the same time
+        mixed = [_submit(srv, r) for r in _mixed_requests(rng, 15)]
+        ids, outs = three()
+        mixed += [_submit(srv, r) for r in _mixed_requests(rng, 15)]
+        infos = [srv.wait(i, WAIT_MS) for i in ids] + [srv.wait(i, WAIT_MS) for i, _ in mixed]
+        assert all(i.status == 0 for i in infos)
+        assert max(i.batch_size for i in infos) > 1
+        for got, ref in zip(outs, (rays_direct, rays_frame, radon_direct)):
+            assert np.array_equal(got, ref)

@@ -54,13 +54,15 @@ class ForwardReq(C.Structure):
                 ("reserved", C.c_int), ("dev_out", C.c_void_p)]
 
 
-OP_FORWARD, OP_ADJOINT = 0, 1
+OP_FORWARD, OP_ADJOINT, OP_RAY, OP_REDUCE = 0, 1, 2, 3
 
 
 class Request(C.Structure):
     _fields_ = [("op", C.c_int), ("ngrid", C.c_int), ("nphi", C.c_int), ("ntheta", C.c_int),
                 ("nshift", C.c_int), ("half_extent", C.c_int), ("volume", C.c_void_p),
-                ("radon", C.c_void_p), ("out", C.c_void_p), ("tag", C.c_uint64)]
+                ("radon", C.c_void_p), ("out", C.c_void_p), ("tag", C.c_uint64),
+                ("nslices", C.c_int), ("nshift_ray", C.c_int), ("rays", C.c_void_p),
+                ("frame", C.c_void_p)]
 
 
 class RequestInfo(C.Structure):
@@ -558,6 +560,29 @@ class Server:
         assert out.flags.c_contiguous and out.dtype == np.float64 and out.size == ngrid ** 3
         r = Request(OP_ADJOINT, int(ngrid), nphi, ntheta, nshift, 0, None, g.ctypes.data,
                     out.ctypes.data, int(tag))
+        return self._submit(r, (g, out))
+
+    def submit_ray(self, volume, nslices, nshift, nphi, out, frame=None, tag=0) -> int:
+        """volume: float32 [n][n][n]; out: float64 [nslices][nshift][nphi]
+        (ray_grid's order); frame: None (z-slices) or a 3x3 rotation."""
+        v = np.ascontiguousarray(volume, dtype=np.float32)
+        assert out.flags.c_contiguous and out.dtype == np.float64
+        assert out.size == nslices * nshift * nphi
+        f = None if frame is None else _f64(frame).reshape(9)
+        r = Request(op=OP_RAY, ngrid=v.shape[0], nphi=int(nphi), ntheta=1, nshift=int(nshift),
+                    volume=v.ctypes.data, out=out.ctypes.data, tag=int(tag),
+                    nslices=int(nslices), frame=None if f is None else f.ctypes.data)
+        return self._submit(r, (v, out, f))
+
+    def submit_reduce(self, rays, nshift, ntheta, out, tag=0) -> int:
+        """rays: float64 [ngrid][nshift_ray][nphi]; out: float64
+        [nshift][nphi][ntheta] on the Gauss-uniform sphere grid."""
+        g = np.ascontiguousarray(rays, dtype=np.float64)
+        ngrid, nsr, nphi = g.shape
+        assert out.flags.c_contiguous and out.dtype == np.float64
+        assert out.size == nshift * nphi * ntheta
+        r = Request(op=OP_REDUCE, ngrid=ngrid, nphi=nphi, ntheta=int(ntheta), nshift=int(nshift),
+                    out=out.ctypes.data, tag=int(tag), nshift_ray=nsr, rays=g.ctypes.data)
         return self._submit(r, (g, out))
 
     def _submit(self, r, keep) -> int:

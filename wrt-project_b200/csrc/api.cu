@@ -90,6 +90,38 @@ int check_launch(wrt_ctx *ctx, const char *what) {
   return WRT_OK;
 }
 
+void ray_tables(int nshift, int nphi, double *tab) {
+  double *shift = tab, *trig = tab + nshift;
+  const double dshift = 2.0 / (nshift - 1);
+  for (int i = 0; i < nshift; ++i) shift[i] = (-1.0) + i * dshift;
+  const double dphi = (2 * M_PI) / nphi;
+  for (int i = 0; i < nphi; ++i) {
+    const double phi = dphi * i;
+    trig[4 * i + 0] = cos(phi);
+    trig[4 * i + 1] = sin(phi);
+    trig[4 * i + 2] = cos(phi + M_PI / 2);
+    trig[4 * i + 3] = sin(phi + M_PI / 2);
+  }
+}
+
+double trilinear_margin(int n) { return sqrt(3.0) * (2.0 / (n - 1)) + 1e-6; }
+
+bool identity_frame(const double *f) {
+  return !f || (f[0] == 1.0 && f[4] == 1.0 && f[8] == 1.0 && f[1] == 0.0 && f[2] == 0.0 &&
+                f[3] == 0.0 && f[5] == 0.0 && f[6] == 0.0 && f[7] == 0.0);
+}
+
+void spline_coefficients(int ns, double *cp, double *den) {
+  for (int i = 0; i < ns; ++i) {
+    cp[i] = 0.0;
+    den[i] = 1.0;
+  }
+  for (int i = 1; i + 1 < ns; ++i) {
+    den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);
+    cp[i] = 1.0 / den[i];
+  }
+}
+
 int ws_get(wrt_ctx *ctx, int role, size_t bytes, void **p) {
   if (role < 0 || role >= WS_ROLES) return fail(ctx, WRT_ERR_INTERNAL, "workspace role %d", role);
   if (bytes <= ctx->ws_bytes[role] && ctx->ws[role]) {
@@ -155,9 +187,9 @@ int set_device(wrt_ctx *ctx) {
 // the sample lies within this distance (trilinear: one cell diagonal of the
 // node grid; nearest: cell 2/n plus the offset between cell and node grids).
 double sampler_margin(int n, int sampler) {
+  if (sampler == WRT_SAMPLER_TRILINEAR) return trilinear_margin(n);
   const double h = 2.0 / (n - 1);
-  const double reach = sampler == WRT_SAMPLER_TRILINEAR ? sqrt(3.0) * h : sqrt(3.0) * (4.0 / n + h);
-  return reach + 1e-6;
+  return sqrt(3.0) * (4.0 / n + h) + 1e-6;
 }
 
 bool valid_plane_opts(const wrt_plane_opts *o, int n) {
@@ -870,22 +902,9 @@ int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const double *f
   int st = set_device(ctx);
   if (st) return st;
   const int n = vol->n;
-  // ray_grid/src/init.c:163-176 and the trig of ray_grid/src/integral.c:16-24
   std::vector<double> tab((size_t)nshift + 4 * (size_t)nphi);
-  double *shift = tab.data(), *trig = tab.data() + nshift;
-  const double dshift = 2.0 / (nshift - 1);
-  for (int i = 0; i < nshift; ++i) shift[i] = (-1.0) + i * dshift;
-  const double dphi = (2 * M_PI) / nphi;
-  for (int i = 0; i < nphi; ++i) {
-    const double phi = dphi * i;
-    trig[4 * i + 0] = cos(phi);
-    trig[4 * i + 1] = sin(phi);
-    trig[4 * i + 2] = cos(phi + M_PI / 2);
-    trig[4 * i + 3] = sin(phi + M_PI / 2);
-  }
-  const bool identity = !frame || (frame[0] == 1.0 && frame[4] == 1.0 && frame[8] == 1.0 &&
-                                   frame[1] == 0.0 && frame[2] == 0.0 && frame[3] == 0.0 &&
-                                   frame[5] == 0.0 && frame[6] == 0.0 && frame[7] == 0.0);
+  ray_tables(nshift, nphi, tab.data());
+  const bool identity = identity_frame(frame);
   void *dtab = nullptr;
   st = ws_get(ctx, WS_TABLE, sizeof(double) * tab.size(), &dtab);
   // a copy from pageable memory returns once the data is staged

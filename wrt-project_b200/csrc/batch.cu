@@ -6,7 +6,8 @@
 // shifts) and kBatchMaxAdj backprojections.  All of it is described by one
 // table in device memory (BatchLayout):
 //
-//   header | StagedReq[kBatchMaxFwd] | FwdAux[kBatchMaxFwd] | AdjReq[kBatchMaxAdj] | items
+//   header | StagedReq[kBatchMaxFwd] | FwdAux[kBatchMaxFwd] | AdjReq[kBatchMaxAdj] |
+//   RayJob[kBatchMaxRay] | RedReq[kBatchMaxRed] | items
 //
 // and executed by one graph, captured once per slot and replayed for every
 // batch (only the size of its first node, the table upload, changes):
@@ -15,7 +16,9 @@
 //   layer pairs of freshly uploaded volumes) -> request prep (crop radius,
 //   fixed-point scale) -> persistent staged plane kernel over the work items
 //   of every forward request, largest first -> finalize (fixed point to FP64)
-//   -> spline prep of every backprojection's lines;
+//   -> spline prep of every backprojection's lines -> every ray of the ray
+//   requests -> spline prep of the reduction requests' ray lines -> every
+//   Radon sample of the reduction requests;
 //
 // then, on the same stream, each backprojection's launches (its direction
 // constants are launch parameters, which a graph replayed unchanged cannot
@@ -24,13 +27,15 @@
 // Every kernel has a fixed grid and reads its work from the table, which is
 // what lets one captured graph serve batches of any composition.  A request's
 // result is bitwise the same alone or in any batch: the plane sums are
-// order-independent fixed-point integers and the backprojection of a voxel is
-// one thread's sequential sum, by the same kernel as a single request's.
+// order-independent fixed-point integers, the backprojection of a voxel is one
+// thread's sequential sum by the same kernel as a single request's, and a ray
+// or a reduced Radon sample is one thread's sum by the single kernel's body.
 #include <string.h>
 
 #include <algorithm>
 #include <vector>
 
+#include "ray_dev.cuh"
 #include "spline_dev.cuh"
 #include "wrt_internal.cuh"
 
@@ -40,6 +45,8 @@ using wrt::AdjReq;
 using wrt::BatchHeader;
 using wrt::BatchLayout;
 using wrt::FwdAux;
+using wrt::RayJob;
+using wrt::RedReq;
 using wrt::StagedReq;
 
 __device__ __forceinline__ const BatchHeader *hdr(const char *t) {
@@ -53,6 +60,19 @@ __device__ __forceinline__ FwdAux *aux_tab(char *t) {
 }
 __device__ __forceinline__ const AdjReq *adj_tab(const char *t) {
   return reinterpret_cast<const AdjReq *>(t + BatchLayout::adj);
+}
+__device__ __forceinline__ const RayJob *ray_tab(const char *t) {
+  return reinterpret_cast<const RayJob *>(t + BatchLayout::ray);
+}
+__device__ __forceinline__ const RedReq *red_tab(const char *t) {
+  return reinterpret_cast<const RedReq *>(t + BatchLayout::red);
+}
+// First index of request r's work for grid thread (or warp) g when the work
+// of consecutive requests is numbered consecutively from `first` and dealt
+// out round-robin over `nth` threads: small requests then leave no thread idle.
+__device__ __forceinline__ long long dealt_first(long long g, long long first, long long nth) {
+  long long k = g - first % nth;
+  return k < 0 ? k + nth : k;
 }
 
 // Zero every forward output (the fixed-point accumulators) and the statistics
@@ -161,7 +181,67 @@ __global__ void batch_spline_kernel(const char *t) {
   }
 }
 
-constexpr int kBatchKernels = 6;  // kernels per graph launch
+// Every ray of every ray-transform request (ray_grid/src/integral.c:11-50):
+// consecutive threads take consecutive rays (32 shifts of one layer and angle).
+__global__ void __launch_bounds__(256) batch_ray_kernel(const char *t) {
+  const int nr = hdr(t)->nray;
+  const RayJob *R = ray_tab(t);
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  long long first = 0;
+  for (int r = 0; r < nr; ++r) {
+    const RayJob &job = R[r];
+    const long long total = (long long)job.nslices * job.nshift * job.nphi;
+    const float g = wrtd::ray_guard(job.n);
+    for (long long k = dealt_first(tid, first, nth); k < total; k += nth) {
+      if (job.has_frame)
+        wrtd::ray_one<true>(job, k, g);
+      else
+        wrtd::ray_one<false>(job, k, g);
+    }
+    first += total;
+  }
+}
+
+// Natural splines of every reduction request's ray lines (one thread per line).
+__global__ void batch_red_spline_kernel(const char *t) {
+  const int nr = hdr(t)->nred;
+  const RedReq *Q = red_tab(t);
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  for (int r = 0; r < nr; ++r) {
+    const RedReq &q = Q[r];
+    const int ns = q.ns_ray, nlines = q.ngrid * q.nphi;
+    // line (iz, iphi): element is at rays[(iz*ns + is)*nphi + iphi]
+    for (long long L = tid; L < nlines; L += nth) {
+      const int outer = (int)(L / q.nphi), inner = (int)(L % q.nphi);
+      wrtd::spline_line(q.rays + (size_t)outer * ns * q.nphi + inner, q.nphi, ns, 2.0 / (ns - 1),
+                        q.coef, q.coef + ns, q.scratch + (size_t)L * ns,
+                        q.lines + (size_t)L * (ns - 1));
+    }
+  }
+}
+
+// Every Radon sample of every reduction request (radon_reduction/slicing.c:80).
+__global__ void __launch_bounds__(256) batch_reduction_kernel(const char *t) {
+  const int nr = hdr(t)->nred;
+  const RedReq *Q = red_tab(t);
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  long long first = 0;
+  for (int r = 0; r < nr; ++r) {
+    const RedReq &q = Q[r];
+    const long long total = (long long)q.nshift * q.nphi * q.ntheta;
+    for (long long k = dealt_first(tid, first, nth); k < total; k += nth) {
+      int evaluated = 0;
+      q.out[k] = wrtd::reduction_one(q.lines, q.ngrid, q.ns_ray, q.nphi, q.shift, q.cs, q.ntheta, k,
+                                     &evaluated);
+    }
+    first += total;
+  }
+}
+
+constexpr int kBatchKernels = 9;  // kernels per graph launch
 
 }  // namespace
 
@@ -267,6 +347,9 @@ int capture(BatchSlot *s) {
   if (!st) {
     batch_finalize_kernel<<<g, 256, 0, s->stream>>>(s->d_table);
     batch_spline_kernel<<<g, 128, 0, s->stream>>>(s->d_table);
+    batch_ray_kernel<<<g, 256, 0, s->stream>>>(s->d_table);
+    batch_red_spline_kernel<<<g, 128, 0, s->stream>>>(s->d_table);
+    batch_reduction_kernel<<<g, 256, 0, s->stream>>>(s->d_table);
     e = cudaGetLastError();
     if (e != cudaSuccess) st = cuda_fail(ctx, e, "batch kernels");
   }
@@ -302,9 +385,11 @@ int capture(BatchSlot *s) {
 
 int batch_slot_launch(BatchSlot *s, BatchBuilder &b) {
   wrt_ctx *ctx = s->ctx;
-  if ((int)b.fwd.size() > kBatchMaxFwd || (int)b.adj.size() > kBatchMaxAdj)
-    return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "batch: more than %d forward or %d adjoint requests",
-                kBatchMaxFwd, kBatchMaxAdj);
+  if ((int)b.fwd.size() > kBatchMaxFwd || (int)b.adj.size() > kBatchMaxAdj ||
+      (int)b.ray.size() > kBatchMaxRay || (int)b.red.size() > kBatchMaxRed)
+    return fail(ctx, WRT_ERR_INVALID_ARGUMENT,
+                "batch: more than %d forward, %d adjoint, %d ray or %d reduction requests",
+                kBatchMaxFwd, kBatchMaxAdj, kBatchMaxRay, kBatchMaxRed);
   // the previous launch of this slot must have consumed the host table
   if (s->launched) {
     cudaError_t e = cudaEventSynchronize(s->done);
@@ -320,7 +405,12 @@ int batch_slot_launch(BatchSlot *s, BatchBuilder &b) {
   std::stable_sort(b.items.begin(), b.items.end(),
                    [](const std::pair<double, StagedItem> &x,
                       const std::pair<double, StagedItem> &y) { return x.first > y.first; });
-  BatchHeader h = {(int)b.fwd.size(), (int)b.adj.size(), (int)b.items.size(), 0};
+  BatchHeader h = {};
+  h.nfwd = (int)b.fwd.size();
+  h.nadj = (int)b.adj.size();
+  h.nitems = (int)b.items.size();
+  h.nray = (int)b.ray.size();
+  h.nred = (int)b.red.size();
   memset(s->h_table, 0, BatchLayout::items);
   memcpy(s->h_table, &h, sizeof(h));
   if (!b.fwd.empty()) {
@@ -329,6 +419,10 @@ int batch_slot_launch(BatchSlot *s, BatchBuilder &b) {
   }
   if (!b.adj.empty())
     memcpy(s->h_table + BatchLayout::adj, b.adj.data(), sizeof(AdjReq) * b.adj.size());
+  if (!b.ray.empty())
+    memcpy(s->h_table + BatchLayout::ray, b.ray.data(), sizeof(RayJob) * b.ray.size());
+  if (!b.red.empty())
+    memcpy(s->h_table + BatchLayout::red, b.red.data(), sizeof(RedReq) * b.red.size());
   StagedItem *items = reinterpret_cast<StagedItem *>(s->h_table + BatchLayout::items);
   for (size_t i = 0; i < b.items.size(); ++i) items[i] = b.items[i].second;
   cudaError_t e = cudaGraphExecMemcpyNodeSetParams1D(s->exec, s->copy_node, s->d_table,

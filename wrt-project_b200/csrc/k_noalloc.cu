@@ -117,14 +117,7 @@ extern "C" int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, i
   wrt::adjoint_directions(nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), h_dirw.data());
   std::vector<double> coef(2 * (size_t)nshift);
   double *h_cp = coef.data(), *h_den = coef.data() + nshift;
-  for (int i = 0; i < nshift; ++i) {
-    h_cp[i] = 0.0;
-    h_den[i] = 1.0;
-  }
-  for (int i = 1; i + 1 < nshift; ++i) {
-    h_den[i] = 4.0 - (i > 1 ? h_cp[i - 1] : 0.0);
-    h_cp[i] = 1.0 / h_den[i];
-  }
+  wrt::spline_coefficients(nshift, h_cp, h_den);
   // copies from pageable host memory return once the data is staged, so the
   // vectors may go out of scope before the copies land
   cudaStream_t s = ctx->stream;

@@ -1,191 +1,14 @@
-// k_ray.cu -- layer-by-layer ray integrals (ray_grid/src/integral.c:11-50).
-//
-// Ray (z, s, phi): p(k) = (s cos phi, s sin phi, z) + delta*k*(cos(phi+pi/2),
-// sin(phi+pi/2), 0), delta = 1/(n-1), k in [-2n, 2n], weight delta, trilinear
-// sampler.  With a frame F every point is mapped to F p(k) (the layer scheme
-// about another axis; F = identity reproduces the reference).
-//
-// One lane per ray; a warp takes 32 consecutive shifts of one (z, phi):
-// parallel rays one shift step apart, whose samples read neighbouring cache
-// lines (2.2x faster than 32 angles of one shift, which fan out).  Samples farther than sqrt(crop_r2) from the origin or outside the
-// cube are skipped (their value is exactly 0).  Numerics: FP32 cell
-// coordinates with the guard band of wrt_internal.cuh.  In the reference
-// frame the z coordinate of a ray is one FP64 number for all its samples, so
-// its cell and fraction are computed once per ray with the reference's own
-// arithmetic (cube_trilinear_interp, radon_grid/src/interp.c:33-53) and used
-// by every FP32 sample of the ray.
-#include "wrt_internal.cuh"
+// k_ray.cu -- layer-by-layer ray integrals (ray_grid/src/integral.c:11-50);
+// the per-ray body is in ray_dev.cuh.
+#include "ray_dev.cuh"
 
 namespace {
-
-__device__ __forceinline__ bool clip_axis(double b, double t, int &lo, int &hi) {
-  const double eps = 1e-13;
-  if (t == 0.0) return fabs(b) <= 1.0 + eps;
-  double k0 = (-1.0 - eps - b) / t, k1 = (1.0 + eps - b) / t;
-  if (k0 > k1) {
-    double s = k0;
-    k0 = k1;
-    k1 = s;
-  }
-  double flo = fmax(floor(k0) - 2.0, (double)lo), fhi = fmin(ceil(k1) + 2.0, (double)hi);
-  if (!(flo <= fhi)) return false;
-  lo = (int)flo;
-  hi = (int)fhi;
-  return true;
-}
-
-__device__ __forceinline__ double rot_row(const double *F, int r, double x, double y, double z) {
-  return __dadd_rn(__dadd_rn(__dmul_rn(F[3 * r], x), __dmul_rn(F[3 * r + 1], y)),
-                   __dmul_rn(F[3 * r + 2], z));
-}
-
-// The 8 corners (x, y, z) .. (x+1, y+1, z+1) of a reference-frame sample:
-// from the layer pairs P[z][y][x] = (v(x,y,z), v(x,y,z+1)) when the volume has
-// them -- a slice reads one z-layer pair, whose rows are contiguous in x, so
-// neighbouring samples share cache lines -- else from the volume v[x][y][z],
-// where a slice uses 2 of the 32 z values of every line it touches.
-struct Corners {
-  const float *vol;
-  const float2 *pairs;
-  int n, pitch;
-  __device__ __forceinline__ void operator()(int ix, int iy, int zc, float c[8]) const {
-    if (pairs) {
-      const float2 *p = pairs + ((size_t)zc * n + iy) * pitch + ix;
-      const float2 a = __ldg(p), b = __ldg(p + pitch), d = __ldg(p + 1), e = __ldg(p + pitch + 1);
-      c[0] = a.x, c[1] = a.y, c[2] = b.x, c[3] = b.y, c[4] = d.x, c[5] = d.y, c[6] = e.x,
-      c[7] = e.y;
-    } else {
-      const float *p = vol + ((size_t)ix * n + iy) * n + zc;
-      const size_t sx = (size_t)n * n;
-      c[0] = __ldg(p), c[1] = __ldg(p + 1), c[2] = __ldg(p + n), c[3] = __ldg(p + n + 1);
-      c[4] = __ldg(p + sx), c[5] = __ldg(p + sx + 1), c[6] = __ldg(p + sx + n);
-      c[7] = __ldg(p + sx + n + 1);
-    }
-  }
-};
 
 template <bool FRAME>
 __global__ void __launch_bounds__(256) ray_kernel(wrt::RayJob job, float guard) {
   const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nrays = (long long)job.nslices * job.nshift * job.nphi;
-  if (ray >= nrays) return;
-  const int is = (int)(ray % job.nshift);
-  const int ip = (int)((ray / job.nshift) % job.nphi);
-  const int iz = (int)(ray / ((long long)job.nphi * job.nshift));
-  const int n = job.n;
-  const Corners corners{job.vol, job.pairs, n, job.pitch};
-  const double *T = job.trig + 4 * ip;
-  const double s = job.shift[is];
-  const double dz = 2.0 / (job.nslices - 1);                     // ray_grid.c:244
-  const double zslice = __dadd_rn(-1.0, __dmul_rn((double)iz, dz));  // ray_grid.c:247
-  const double delta = (2.0 / (n - 1)) / (2.0);                  // integral.c:32
-  const double p0x = __dmul_rn(s, T[0]), p0y = __dmul_rn(s, T[1]), p0z = zslice;
-  const double ax = __dmul_rn(delta, T[2]), ay = __dmul_rn(delta, T[3]);  // delta*direction
-  double acc = 0.0;
-
-  double crop_r2 = 3.0 + 1e-9;
-  if (job.r2bits) {
-    const double r = sqrt((double)__uint_as_float(__ldg(job.r2bits))) + job.margin;
-    crop_r2 = fmin(r * r, crop_r2);
-  }
-  const double rem = crop_r2 - s * s - zslice * zslice;
-  const int half = 2 * n;  // nsize/2 with nsize = 4n
-  int klo = -half, khi = half;
-  bool any = rem >= 0.0;
-  if (any) {
-    int km = (int)floor(sqrt(rem) / delta) + 1;
-    klo = max(klo, -km);
-    khi = min(khi, km);
-    any = klo <= khi;
-  }
-  const double h = 0.5 * (n - 1);
-  const float qmax = (float)(n - 1);
-  const double *F = job.frame;  // kernel parameter space
-  if (any && !FRAME) {
-    any = clip_axis(p0x, ax, klo, khi) && clip_axis(p0y, ay, klo, khi) && fabs(zslice) <= 1.0;
-  } else if (any) {
-    double bx = rot_row(F, 0, p0x, p0y, p0z), by = rot_row(F, 1, p0x, p0y, p0z),
-           bz = rot_row(F, 2, p0x, p0y, p0z);
-    double tx = F[0] * ax + F[1] * ay, ty = F[3] * ax + F[4] * ay, tz = F[6] * ax + F[7] * ay;
-    any = clip_axis(bx, tx, klo, khi) && clip_axis(by, ty, klo, khi) && clip_axis(bz, tz, klo, khi);
-  }
-  if (any) {
-    float ub, vb, wb, du, dv, dw;
-    int zc = 0;
-    float tzc = 0.0f;
-    if (!FRAME) {
-      ub = (float)((p0x + 1.0) * h);
-      vb = (float)((p0y + 1.0) * h);
-      du = (float)(ax * h);
-      dv = (float)(ay * h);
-      wb = 0.0f;
-      dw = 0.0f;
-      // z cell of the whole ray, reference arithmetic (interp.c:32-53)
-      const double dlt = 2.0 / (n - 1);
-      const double z1 = __dadd_rn(zslice, 1.0);
-      zc = (int)__ddiv_rn(z1, dlt);
-      double cz = __ddiv_rn(fmod(z1, dlt), dlt);
-      if (zc == n - 1) {
-        zc -= 1;
-        cz = 1.0;
-      }
-      tzc = (float)cz;
-    } else {
-      const double bx = rot_row(F, 0, p0x, p0y, p0z), by = rot_row(F, 1, p0x, p0y, p0z),
-                   bz = rot_row(F, 2, p0x, p0y, p0z);
-      ub = (float)((bx + 1.0) * h);
-      vb = (float)((by + 1.0) * h);
-      wb = (float)((bz + 1.0) * h);
-      du = (float)((F[0] * ax + F[1] * ay) * h);
-      dv = (float)((F[3] * ax + F[4] * ay) * h);
-      dw = (float)((F[6] * ax + F[7] * ay) * h);
-    }
-    for (int k0 = klo; k0 <= khi; k0 += 32) {
-      const int k1 = min(khi, k0 + 31);
-      float part = 0.0f;
-      for (int k = k0; k <= k1; ++k) {
-        const float kf = (float)k;
-        const float qx = fmaf(kf, du, ub), qy = fmaf(kf, dv, vb);
-        const float qz = FRAME ? fmaf(kf, dw, wb) : 0.5f;
-        bool band = wrtd::in_band(qx, guard) | wrtd::in_band(qy, guard);
-        if (FRAME) band |= wrtd::in_band(qz, guard);
-        if (band) {
-          const double dk = (double)k;
-          double px = __dadd_rn(p0x, __dmul_rn(ax, dk));
-          double py = __dadd_rn(p0y, __dmul_rn(ay, dk));
-          double pz = __dadd_rn(p0z, __dmul_rn(__dmul_rn(delta, 0.0), dk));
-          if (FRAME) {
-            double wx = rot_row(F, 0, px, py, pz), wy = rot_row(F, 1, px, py, pz),
-                   wz = rot_row(F, 2, px, py, pz);
-            px = wx;
-            py = wy;
-            pz = wz;
-          }
-          acc += wrtd::exact_trilinear(job.vol, n, px, py, pz);
-        } else if (qx > 0.0f && qy > 0.0f && qx < qmax && qy < qmax &&
-                   (!FRAME || (qz > 0.0f && qz < qmax))) {
-          if (FRAME) {
-            part += wrtd::tri32(job.vol, n, qx, qy, qz);
-          } else {
-            // bilinear in x, y on layers zc and zc+1, then the ray's z weight
-            const float fx = floorf(qx), fy = floorf(qy);
-            const float tx = qx - fx, ty = qy - fy;
-            float c[8];
-            corners((int)fx, (int)fy, zc, c);
-            const float c000 = c[0], c001 = c[1], c010 = c[2], c011 = c[3], c100 = c[4],
-                        c101 = c[5], c110 = c[6], c111 = c[7];
-            const float a0 = wrtd::lerp32(tx, c000, c100), a1 = wrtd::lerp32(tx, c010, c110);
-            const float b0 = wrtd::lerp32(tx, c001, c101), b1 = wrtd::lerp32(tx, c011, c111);
-            const float e0 = wrtd::lerp32(ty, a0, a1), e1 = wrtd::lerp32(ty, b0, b1);
-            part += wrtd::lerp32(tzc, e0, e1);
-          }
-        }
-      }
-      acc += (double)part;
-    }
-  }
-  if (job.counter && any) atomicAdd(job.counter, (unsigned long long)(khi - klo + 1));
-  job.out[((long long)iz * job.nshift + is) * job.nphi + ip] = acc * delta;
+  if (ray >= (long long)job.nslices * job.nshift * job.nphi) return;
+  wrtd::ray_one<FRAME>(job, ray, guard);
 }
 
 }  // namespace
@@ -197,7 +20,7 @@ int ray_forward(wrt_ctx *ctx, const RayJob &job) {
   if (nrays == 0) return WRT_OK;
   const long long blocks = (nrays + 255) / 256;
   if (blocks > 0x7fffffffLL) return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "too many rays");
-  const float g = 4.8e-7f * (float)(job.n > 64 ? job.n : 64);
+  const float g = wrtd::ray_guard(job.n);
   if (job.has_frame)
     ray_kernel<true><<<(unsigned)blocks, 256, 0, ctx->stream>>>(job, g);
   else

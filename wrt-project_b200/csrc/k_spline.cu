@@ -42,66 +42,17 @@ __global__ void spline_prep_kernel(const double *__restrict__ src, int nlines, i
                       out + (size_t)L * (ns - 1));
 }
 
-// Reduction: one thread per Radon sample (is, iphi, itheta), order of
-// reduction.c:215-229.  Geometry in FP64 with the reference's expressions;
-// spline values and the quadratic in FP32.
+// Reduction: one thread per Radon sample (wrtd::reduction_one).
 __global__ void __launch_bounds__(256)
     reduction_kernel(const float4 *__restrict__ lines /* [iz][iphi][ns_ray-1] */, int ngrid,
                      int ns_ray, int nphi, const double *__restrict__ shift, int nshift,
                      const double *__restrict__ cs /* [ntheta][2] cos, sin */, int ntheta,
                      double *__restrict__ out, unsigned long long *counter) {
   const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long total = (long long)nshift * nphi * ntheta;
-  if (k >= total) return;
-  const int it = (int)(k % ntheta), ip = (int)((k / ntheta) % nphi),
-            is = (int)(k / ((long long)ntheta * nphi));
-  const double p = shift[is], ct = cs[2 * it], st = cs[2 * it + 1];
-  const double dtau = (2.0 / (ngrid - 1)) / (2.0);  // slicing.c:88
-  const double delta_z = 2.0 / (ngrid - 1);         // slicing.c:18
-  const double inv_dz = 0.5 * (ngrid - 1);
-  const float hs = 2.0f / (float)(ns_ray - 1);
-  const float inv_hs = 1.0f / hs;
-  const float h2_6 = hs * hs / 6.0f;
-  const int half = 2 * ngrid;
-  // |tau| <= sqrt(1 - p^2) bounds the samples that pass slicing.c:110
-  int kmax = half;
-  {
-    double r = 1.0 - p * p;
-    if (r < 0.0) kmax = -1;
-    else kmax = min(half, (int)floor(sqrt(r) / dtau) + 1);
-  }
-  double acc = 0.0;
+  if (k >= (long long)nshift * nphi * ntheta) return;
   int evaluated = 0;
-  const size_t line_len = (size_t)(ns_ray - 1);
-  for (int itau = -kmax; itau <= kmax; ++itau) {
-    const double tau = __dmul_rn((double)itau, dtau);
-    const double z = __dadd_rn(__dmul_rn(p, ct), __dmul_rn(tau, st));
-    const double s = __dsub_rn(__dmul_rn(p, st), __dmul_rn(tau, ct));
-    if ((fabs(__dadd_rn(__dmul_rn(tau, tau), __dmul_rn(p, p))) > 1.0) || (fabs(z) > 1.0) ||
-        (fabs(s) > 1.0))
-      continue;
-    // layer index of slicing.c:15-20, (int)((z + 1) / delta_z): by the
-    // reciprocal, and by the division itself where the quotient lies within
-    // 1e-9 of an integer (the reciprocal's error is ~1e-14 there)
-    const double z1 = __dadd_rn(z, 1.0), qz = z1 * inv_dz;
-    int iz = (int)qz;
-    if (fabs(qz - rint(qz)) < 1e-9) iz = (int)__ddiv_rn(z1, delta_z);
-    if (iz == ngrid - 1) iz -= 1;
-    const double z0 = __dadd_rn(-1.0, __dmul_rn(delta_z, (double)iz));
-    const float f = (float)((z - z0) * inv_dz);
-    const float q = (float)(s + 1.0) * inv_hs;
-    const float4 *l0 = lines + ((size_t)iz * nphi + ip) * line_len;
-    const float v0 = wrtd::spline_eval(l0, ns_ray, q, h2_6);
-    const float v1 = wrtd::spline_eval(l0 + (size_t)nphi * line_len, ns_ray, q, h2_6);
-    const float v2 =
-        iz >= ngrid - 2 ? 0.0f : wrtd::spline_eval(l0 + 2 * (size_t)nphi * line_len, ns_ray, q, h2_6);
-    // quadratic through (z0, v0), (z0+dz, v1), (z0+2dz, v2) at z0 + f dz
-    const float val = v0 + f * (v1 - v0) + 0.5f * f * (f - 1.0f) * (v2 - 2.0f * v1 + v0);
-    acc += (double)val;
-    ++evaluated;
-  }
+  out[k] = wrtd::reduction_one(lines, ngrid, ns_ray, nphi, shift, cs, ntheta, k, &evaluated);
   if (counter) atomicAdd(counter, (unsigned long long)evaluated);
-  out[k] = acc * dtau;
 }
 
 // Adjoint: one warp per voxel block of wrtd::adjoint_block (8 x 4 columns of
@@ -125,12 +76,7 @@ int prep_lines(wrt_ctx *ctx, const double *d_src, int nlines, int ninner, long l
   // h M_{i-1} + 4h M_i + h M_{i+1} = rhs (divided by h: M_{i-1} + 4 M_i + M_{i+1})
   const double h = 2.0 / (ns - 1);
   std::vector<double> coef(2 * (size_t)ns, 0.0);
-  double *cp = coef.data(), *den = coef.data() + ns;
-  for (int i = 0; i < ns; ++i) den[i] = 1.0;
-  for (int i = 1; i + 1 < ns; ++i) {
-    den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);
-    cp[i] = 1.0 / den[i];
-  }
+  wrt::spline_coefficients(ns, coef.data(), coef.data() + ns);
   void *d_coef = nullptr, *d_scratch = nullptr, *lines = nullptr;
   int st = wrt::ws_get(ctx, wrt::WS_COEF, sizeof(double) * coef.size(), &d_coef);
   if (!st) st = wrt::ws_get(ctx, wrt::WS_SPLINE, sizeof(double) * (size_t)nlines * ns, &d_scratch);

@@ -56,6 +56,7 @@ struct GridTables {
   double4 *dirw = nullptr;   // [ndir]
   std::vector<double4> h_dirw;  // host copy (backprojection launch parameters)
   double *cp = nullptr, *den = nullptr;  // [nshift]
+  double *cs = nullptr;      // [ntheta][2]: cos, sin theta (reduction)
   int nphi = 0, ntheta = 0, nshift = 0;
   int refs = 0;
   uint64_t last_use = 0;
@@ -76,6 +77,12 @@ struct Request {
   void *d_in = nullptr;
   double *d_out = nullptr;
   size_t in_bytes = 0, out_bytes = 0;
+  // ray and reduce requests: small host tables uploaded beside the input
+  // (ray: shifts and trig; reduce: spline coefficients) and the ray frame
+  std::vector<double> tab;
+  void *d_tab = nullptr;
+  double frame[9] = {};
+  bool has_frame = false;
 };
 
 struct Slot {
@@ -116,12 +123,21 @@ namespace {
 // ---------------------------------------------------------------- sizes
 size_t forward_pitch(int n) { return (size_t)n + (n & 1); }
 
+size_t ray_table_len(const wrt_request &r) { return (size_t)r.nshift + 4 * (size_t)r.nphi; }
+
 size_t request_bytes(const wrt_request &r) {
   const size_t nplanes = (size_t)r.nphi * r.ntheta * r.nshift;
   const size_t n = (size_t)r.ngrid;
-  if (r.op == WRT_OP_FORWARD)
-    return al(4 * n * n * n) + al(8 * (n - 1) * n * forward_pitch((int)n)) + al(8) +
-           al(8 * nplanes);
+  const size_t vol_state = al(4 * n * n * n) + al(8 * (n - 1) * n * forward_pitch((int)n)) + al(8);
+  if (r.op == WRT_OP_FORWARD) return vol_state + al(8 * nplanes);
+  if (r.op == WRT_OP_RAY)
+    return vol_state + al(8 * ray_table_len(r)) +
+           al(8 * (size_t)r.nslices * r.nshift * r.nphi);
+  if (r.op == WRT_OP_REDUCE) {
+    const size_t nlines = n * r.nphi, nsr = (size_t)r.nshift_ray;
+    return al(8 * nlines * nsr) + al(16 * nsr) + al(8 * nlines * nsr) +
+           al(16 * nlines * (nsr - 1)) + al(8 * nplanes);
+  }
   const size_t ndir = (size_t)r.nphi * r.ntheta;
   return al(8 * nplanes) + al(8 * ndir * r.nshift) + al(16 * ndir * (r.nshift - 1)) +
          al(8 * n * n * n);
@@ -130,7 +146,7 @@ size_t request_bytes(const wrt_request &r) {
 size_t grid_bytes(int nphi, int ntheta, int nshift) {
   const size_t ndir = (size_t)nphi * ntheta;
   return al(72 * ndir) + al(32 * ndir) + al(8 * (size_t)nshift) + al(4 * (size_t)nshift) +
-         al(32 * ndir) + 2 * al(8 * (size_t)nshift);
+         al(32 * ndir) + 2 * al(8 * (size_t)nshift) + al(16 * (size_t)ntheta);
 }
 
 // ---------------------------------------------------------------- grids
@@ -153,10 +169,12 @@ int make_grid(wrt_server *s, GridTables &g) {
   std::vector<double4> &dirw = g.h_dirw;
   dirw.resize(ndir);
   wrt::adjoint_directions(nphi, ntheta, nshift, phi.data(), theta.data(), w.data(), dirw.data());
-  std::vector<double> cp(nshift, 0.0), den(nshift, 1.0);
-  for (int i = 1; i + 1 < nshift; ++i) {
-    den[i] = 4.0 - (i > 1 ? cp[i - 1] : 0.0);
-    cp[i] = 1.0 / den[i];
+  std::vector<double> cp(nshift), den(nshift);
+  wrt::spline_coefficients(nshift, cp.data(), den.data());
+  std::vector<double> cs(2 * (size_t)ntheta);
+  for (int i = 0; i < ntheta; ++i) {
+    cs[2 * i] = cos(theta[i]);  // slicing.c:104-105 evaluate cos/sin(p_theta)
+    cs[2 * i + 1] = sin(theta[i]);
   }
   char *b = s->arena_base + g.off;
   size_t o = 0;
@@ -172,6 +190,7 @@ int make_grid(wrt_server *s, GridTables &g) {
   g.dirw = reinterpret_cast<double4 *>(place(32 * ndir));
   g.cp = reinterpret_cast<double *>(place(8 * (size_t)nshift));
   g.den = reinterpret_cast<double *>(place(8 * (size_t)nshift));
+  g.cs = reinterpret_cast<double *>(place(16 * (size_t)ntheta));
   struct {
     void *dst;
     const void *src;
@@ -179,7 +198,7 @@ int make_grid(wrt_server *s, GridTables &g) {
   } copies[] = {{g.dir, dir.data(), 72 * ndir},          {g.dir32, dir32.data(), 32 * ndir},
                 {g.shift, shift.data(), 8 * (size_t)nshift}, {g.shift32, shift32.data(), 4 * (size_t)nshift},
                 {g.dirw, dirw.data(), 32 * ndir},         {g.cp, cp.data(), 8 * (size_t)nshift},
-                {g.den, den.data(), 8 * (size_t)nshift}};
+                {g.den, den.data(), 8 * (size_t)nshift},  {g.cs, cs.data(), 16 * (size_t)ntheta}};
   for (auto &c : copies) {
     cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "server grid tables");
@@ -233,17 +252,18 @@ GridTables *acquire_grid(wrt_server *s, const wrt_request &r, int *status) {
 // Reserves a request's state in the arena.  Caller holds s->mu.
 bool reserve(wrt_server *s, Request *q, int *status) {
   *status = WRT_OK;
-  GridTables *g = acquire_grid(s, q->req, status);
-  if (!g) return false;
+  const bool needs_grid = q->req.op != WRT_OP_RAY;
+  GridTables *g = needs_grid ? acquire_grid(s, q->req, status) : nullptr;
+  if (needs_grid && !g) return false;
   const size_t bytes = request_bytes(q->req);
   size_t off = 0;
   if (!s->arena.alloc(bytes, &off)) {
-    g->refs--;
+    if (g) g->refs--;
     evict_unused_grids(s);
-    g = acquire_grid(s, q->req, status);
-    if (!g) return false;
+    g = needs_grid ? acquire_grid(s, q->req, status) : nullptr;
+    if (needs_grid && !g) return false;
     if (!s->arena.alloc(bytes, &off)) {
-      g->refs--;
+      if (g) g->refs--;
       return false;
     }
   }
@@ -255,12 +275,30 @@ bool reserve(wrt_server *s, Request *q, int *status) {
   const size_t nplanes = (size_t)r.nphi * r.ntheta * r.nshift;
   const size_t n = (size_t)r.ngrid;
   char *b = s->arena_base + off;
+  const size_t vol_state = al(4 * n * n * n) + al(8 * (n - 1) * n * forward_pitch((int)n)) + al(8);
   if (r.op == WRT_OP_FORWARD) {
     q->d_in = b;  // volume, then pairs, stats, output
     q->in_bytes = 4 * n * n * n;
     q->out_bytes = 8 * nplanes;
-    q->d_out = reinterpret_cast<double *>(b + al(4 * n * n * n) +
-                                          al(8 * (n - 1) * n * forward_pitch((int)n)) + al(8));
+    q->d_out = reinterpret_cast<double *>(b + vol_state);
+  } else if (r.op == WRT_OP_RAY) {
+    q->d_in = b;  // volume, then pairs, stats, tables, output
+    q->in_bytes = 4 * n * n * n;
+    q->d_tab = b + vol_state;
+    q->tab.resize(ray_table_len(r));
+    wrt::ray_tables(r.nshift, r.nphi, q->tab.data());
+    q->out_bytes = 8 * (size_t)r.nslices * r.nshift * r.nphi;
+    q->d_out = reinterpret_cast<double *>(b + vol_state + al(8 * ray_table_len(r)));
+  } else if (r.op == WRT_OP_REDUCE) {
+    const size_t nlines = n * r.nphi, nsr = (size_t)r.nshift_ray;
+    q->d_in = b;  // ray data, then spline coefficients, scratch, lines, output
+    q->in_bytes = 8 * nlines * nsr;
+    q->d_tab = b + al(8 * nlines * nsr);
+    q->tab.resize(2 * nsr);
+    wrt::spline_coefficients((int)nsr, q->tab.data(), q->tab.data() + nsr);
+    q->out_bytes = 8 * nplanes;
+    q->d_out = reinterpret_cast<double *>(b + al(8 * nlines * nsr) + al(16 * nsr) +
+                                          al(8 * nlines * nsr) + al(16 * nlines * (nsr - 1)));
   } else {
     const size_t ndir = (size_t)r.nphi * r.ntheta;
     q->d_in = b;  // radon data, then spline scratch, lines, output
@@ -295,6 +333,67 @@ void add_to_batch(wrt_server *s, Request *q, wrt::BatchBuilder &b) {
   const int n = r.ngrid;
   const int ndir = r.nphi * r.ntheta;
   char *base = static_cast<char *>(q->d_in);
+  if (r.op == WRT_OP_RAY) {
+    // the volume is prepared (statistics, layer pairs) by the batch's volume
+    // kernel through a forward entry with no planes and no work items
+    const size_t nn = (size_t)n;
+    float *vol = reinterpret_cast<float *>(base);
+    float2 *pairs = reinterpret_cast<float2 *>(base + al(4 * nn * nn * nn));
+    unsigned int *stats = reinterpret_cast<unsigned int *>(
+        base + al(4 * nn * nn * nn) + al(8 * (nn - 1) * nn * forward_pitch(n)));
+    wrt::StagedReq sr;
+    wrt::staged_request(n, (int)forward_pitch(n), 0, 0, 2 * n, WRT_STORAGE_F32, pairs, vol,
+                        nullptr, nullptr, nullptr, nullptr, nullptr, &sr);
+    wrt::FwdAux a = {};
+    a.vol = vol;
+    a.pairs = pairs;
+    a.stats = stats;
+    a.nout = 0;
+    a.n = n;
+    a.pitch = (int)forward_pitch(n);
+    a.L = 2 * n;
+    a.prep = 1;
+    b.fwd.push_back(sr);
+    b.aux.push_back(a);
+    wrt::RayJob job = {};
+    job.vol = vol;
+    job.n = n;
+    job.nslices = r.nslices;
+    job.nshift = r.nshift;
+    job.nphi = r.nphi;
+    job.shift = static_cast<const double *>(q->d_tab);
+    job.trig = static_cast<const double *>(q->d_tab) + r.nshift;
+    job.has_frame = q->has_frame ? 1 : 0;
+    for (int k = 0; k < 9; ++k) job.frame[k] = q->frame[k];
+    job.r2bits = stats;
+    job.margin = wrt::trilinear_margin(n);
+    job.out = q->d_out;
+    if (!q->has_frame) {  // z-slices read the layer pairs
+      job.pairs = pairs;
+      job.pitch = (int)forward_pitch(n);
+    }
+    b.ray.push_back(job);
+    return;
+  }
+  if (r.op == WRT_OP_REDUCE) {
+    const size_t nlines = (size_t)n * r.nphi, nsr = (size_t)r.nshift_ray;
+    wrt::RedReq rq = {};
+    rq.rays = reinterpret_cast<const double *>(base);
+    rq.coef = static_cast<const double *>(q->d_tab);
+    rq.scratch = reinterpret_cast<double *>(base + al(8 * nlines * nsr) + al(16 * nsr));
+    rq.lines = reinterpret_cast<float4 *>(base + al(8 * nlines * nsr) + al(16 * nsr) +
+                                          al(8 * nlines * nsr));
+    rq.shift = g->shift;
+    rq.cs = g->cs;
+    rq.out = q->d_out;
+    rq.ngrid = n;
+    rq.ns_ray = (int)nsr;
+    rq.nphi = r.nphi;
+    rq.nshift = r.nshift;
+    rq.ntheta = r.ntheta;
+    b.red.push_back(rq);
+    return;
+  }
   if (r.op == WRT_OP_FORWARD) {
     const size_t nn = (size_t)n;
     float *vol = reinterpret_cast<float *>(base);
@@ -365,11 +464,14 @@ void dispatch_loop(wrt_server *s) {
     // ---- admit in arrival order while memory allows
     std::vector<Request *> batch;
     const int max_batch = s->opts.max_batch;
-    int nfwd = 0, nadj = 0;
+    int nfwd = 0, nadj = 0, nray = 0, nred = 0;  // forward slots include ray volumes
     while (!s->arrivals.empty() && (int)batch.size() < max_batch) {
       Request *q = s->arrivals.front();
-      if ((q->req.op == WRT_OP_FORWARD && nfwd >= wrt::kBatchMaxFwd) ||
-          (q->req.op == WRT_OP_ADJOINT && nadj >= wrt::kBatchMaxAdj))
+      const int op = q->req.op;
+      if (((op == WRT_OP_FORWARD || op == WRT_OP_RAY) && nfwd >= wrt::kBatchMaxFwd) ||
+          (op == WRT_OP_ADJOINT && nadj >= wrt::kBatchMaxAdj) ||
+          (op == WRT_OP_RAY && nray >= wrt::kBatchMaxRay) ||
+          (op == WRT_OP_REDUCE && nred >= wrt::kBatchMaxRed))
         break;
       int st = WRT_OK;
       if (!reserve(s, q, &st)) {
@@ -379,7 +481,10 @@ void dispatch_loop(wrt_server *s) {
         continue;
       }
       s->arrivals.pop_front();
-      (q->req.op == WRT_OP_FORWARD ? nfwd : nadj)++;
+      if (op == WRT_OP_FORWARD || op == WRT_OP_RAY) ++nfwd;
+      if (op == WRT_OP_ADJOINT) ++nadj;
+      if (op == WRT_OP_RAY) ++nray;
+      if (op == WRT_OP_REDUCE) ++nred;
       batch.push_back(q);
     }
     if (batch.empty()) {
@@ -397,10 +502,16 @@ void dispatch_loop(wrt_server *s) {
       q->t_start = t_start;
       q->batch_size = (int)batch.size();
       q->out_pinned = is_pinned(q->req.out);
-      const void *src = q->req.op == WRT_OP_FORWARD ? (const void *)q->req.volume
-                                                    : (const void *)q->req.radon;
+      const int op = q->req.op;
+      const void *src = (op == WRT_OP_FORWARD || op == WRT_OP_RAY) ? (const void *)q->req.volume
+                        : op == WRT_OP_REDUCE                     ? (const void *)q->req.rays
+                                                                  : (const void *)q->req.radon;
       cudaError_t e = cudaMemcpyAsync(q->d_in, src, q->in_bytes, cudaMemcpyHostToDevice,
                                       slot->stream);
+      // small tables from pageable memory: staged before the call returns
+      if (e == cudaSuccess && !q->tab.empty())
+        e = cudaMemcpyAsync(q->d_tab, q->tab.data(), sizeof(double) * q->tab.size(),
+                            cudaMemcpyHostToDevice, slot->stream);
       if (e != cudaSuccess && !st) st = wrt::cuda_fail(s->ctx, e, "server input upload");
       add_to_batch(s, q, b);
     }
@@ -484,7 +595,8 @@ int wrt_server_create(const wrt_server_opts *opts, wrt_server **out) {
   wrt_server_opts o = {};
   if (opts) o = *opts;
   if (o.max_batch <= 0) o.max_batch = 64;
-  if (o.max_batch > wrt::kBatchMaxFwd + wrt::kBatchMaxAdj) o.max_batch = wrt::kBatchMaxFwd + wrt::kBatchMaxAdj;
+  const int most = wrt::kBatchMaxFwd + wrt::kBatchMaxAdj + wrt::kBatchMaxRed;
+  if (o.max_batch > most) o.max_batch = most;
   if (o.max_inflight <= 0) o.max_inflight = 2;
   if (o.max_inflight > 8) o.max_inflight = 8;
   if (o.queue_capacity <= 0) o.queue_capacity = 1 << 16;
@@ -542,10 +654,19 @@ int wrt_server_create(const wrt_server_opts *opts, wrt_server **out) {
 int wrt_server_submit(wrt_server *s, const wrt_request *r, uint64_t *id) {
   if (!s || !r || !id) return WRT_ERR_INVALID_ARGUMENT;
   *id = 0;
-  if (r->op != WRT_OP_FORWARD && r->op != WRT_OP_ADJOINT) return WRT_ERR_INVALID_ARGUMENT;
-  if (r->nphi < 1 || r->ntheta < 1 || !r->out) return WRT_ERR_INVALID_ARGUMENT;
-  if ((long long)r->nphi * r->ntheta > (1 << 24)) return WRT_ERR_INVALID_ARGUMENT;
-  if (r->op == WRT_OP_FORWARD) {
+  if (r->op < WRT_OP_FORWARD || r->op > WRT_OP_REDUCE) return WRT_ERR_INVALID_ARGUMENT;
+  if (r->nphi < 1 || (r->op != WRT_OP_RAY && r->ntheta < 1) || !r->out)
+    return WRT_ERR_INVALID_ARGUMENT;
+  if ((long long)r->nphi * (r->op == WRT_OP_RAY ? 1 : r->ntheta) > (1 << 24))
+    return WRT_ERR_INVALID_ARGUMENT;
+  if (r->op == WRT_OP_RAY) {
+    if (!r->volume || r->ngrid < 4 || r->ngrid > 2048 || r->nslices < 2 || r->nshift < 2 ||
+        (long long)r->nslices * r->nshift * r->nphi > (1LL << 34))
+      return WRT_ERR_INVALID_ARGUMENT;
+  } else if (r->op == WRT_OP_REDUCE) {
+    if (!r->rays || r->ngrid < 3 || r->ngrid > 4096 || r->nshift_ray < 3 || r->nshift < 2)
+      return WRT_ERR_INVALID_ARGUMENT;
+  } else if (r->op == WRT_OP_FORWARD) {
     int th = 0, qp = 0;
     if (!r->volume || r->ngrid < 4 || r->ngrid > 2048 || r->nshift < 2 ||
         wrt::staged_smem_bytes(r->ngrid, &th, &qp) <= 0 || r->half_extent < 0 ||
@@ -554,9 +675,15 @@ int wrt_server_submit(wrt_server *s, const wrt_request *r, uint64_t *id) {
   } else {
     if (!r->radon || r->ngrid < 1 || r->ngrid > 2048 || r->nshift < 3) return WRT_ERR_INVALID_ARGUMENT;
   }
-  const size_t need = request_bytes(*r) + grid_bytes(r->nphi, r->ntheta, r->nshift);
+  const size_t need = request_bytes(*r) +
+                      (r->op == WRT_OP_RAY ? 0 : grid_bytes(r->nphi, r->ntheta, r->nshift));
   auto q = std::make_unique<Request>();
   q->req = *r;
+  if (r->op == WRT_OP_RAY && r->frame && !wrt::identity_frame(r->frame)) {
+    q->has_frame = true;
+    memcpy(q->frame, r->frame, sizeof(q->frame));
+  }
+  q->req.frame = nullptr;  // read here; the caller's array may go away
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->stop) return WRT_ERR_CANCELLED;
   if (need > s->arena.capacity()) return WRT_ERR_BUDGET;

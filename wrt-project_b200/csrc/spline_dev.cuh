@@ -88,6 +88,68 @@ __device__ __forceinline__ float cubic_centred(const float4 c, float u) {
   return fmaf(u, fmaf(u, fmaf(u, c.w, c.z), c.y), c.x);
 }
 
+// ------------------------------------------------------------ reduction
+// radon_reduction (radon_reduction/slicing.c:80-119) of Radon sample k
+// (is, iphi, itheta), order of reduction.c:215-229, from the reduction lines
+// [iz][iphi][ns_ray-1] of the ray data: geometry in FP64 with the reference's
+// expressions, spline values and the quadratic in z (slicing.c:62-74) in
+// FP32.  Returns the integral; *evaluated counts the slice samples taken.
+__device__ __forceinline__ double reduction_one(const float4 *__restrict__ lines, int ngrid,
+                                                int ns_ray, int nphi,
+                                                const double *__restrict__ shift,
+                                                const double *__restrict__ cs, int ntheta,
+                                                long long k, int *evaluated_out) {
+  const int it = (int)(k % ntheta), ip = (int)((k / ntheta) % nphi),
+            is = (int)(k / ((long long)ntheta * nphi));
+  const double p = shift[is], ct = cs[2 * it], st = cs[2 * it + 1];
+  const double dtau = (2.0 / (ngrid - 1)) / (2.0);  // slicing.c:88
+  const double delta_z = 2.0 / (ngrid - 1);         // slicing.c:18
+  const double inv_dz = 0.5 * (ngrid - 1);
+  const float hs = 2.0f / (float)(ns_ray - 1);
+  const float inv_hs = 1.0f / hs;
+  const float h2_6 = hs * hs / 6.0f;
+  const int half = 2 * ngrid;
+  // |tau| <= sqrt(1 - p^2) bounds the samples that pass slicing.c:110
+  int kmax = half;
+  {
+    double r = 1.0 - p * p;
+    if (r < 0.0) kmax = -1;
+    else kmax = min(half, (int)floor(sqrt(r) / dtau) + 1);
+  }
+  double acc = 0.0;
+  int evaluated = 0;
+  const size_t line_len = (size_t)(ns_ray - 1);
+  for (int itau = -kmax; itau <= kmax; ++itau) {
+    const double tau = __dmul_rn((double)itau, dtau);
+    const double z = __dadd_rn(__dmul_rn(p, ct), __dmul_rn(tau, st));
+    const double s = __dsub_rn(__dmul_rn(p, st), __dmul_rn(tau, ct));
+    if ((fabs(__dadd_rn(__dmul_rn(tau, tau), __dmul_rn(p, p))) > 1.0) || (fabs(z) > 1.0) ||
+        (fabs(s) > 1.0))
+      continue;
+    // layer index of slicing.c:15-20, (int)((z + 1) / delta_z): by the
+    // reciprocal, and by the division itself where the quotient lies within
+    // 1e-9 of an integer (the reciprocal's error is ~1e-14 there)
+    const double z1 = __dadd_rn(z, 1.0), qz = z1 * inv_dz;
+    int iz = (int)qz;
+    if (fabs(qz - rint(qz)) < 1e-9) iz = (int)__ddiv_rn(z1, delta_z);
+    if (iz == ngrid - 1) iz -= 1;
+    const double z0 = __dadd_rn(-1.0, __dmul_rn(delta_z, (double)iz));
+    const float f = (float)((z - z0) * inv_dz);
+    const float q = (float)(s + 1.0) * inv_hs;
+    const float4 *l0 = lines + ((size_t)iz * nphi + ip) * line_len;
+    const float v0 = spline_eval(l0, ns_ray, q, h2_6);
+    const float v1 = spline_eval(l0 + (size_t)nphi * line_len, ns_ray, q, h2_6);
+    const float v2 =
+        iz >= ngrid - 2 ? 0.0f : spline_eval(l0 + 2 * (size_t)nphi * line_len, ns_ray, q, h2_6);
+    // quadratic through (z0, v0), (z0+dz, v1), (z0+2dz, v2) at z0 + f dz
+    const float val = v0 + f * (v1 - v0) + 0.5f * f * (f - 1.0f) * (v2 - 2.0f * v1 + v0);
+    acc += (double)val;
+    ++evaluated;
+  }
+  *evaluated_out = evaluated;
+  return acc * dtau;
+}
+
 // ------------------------------------------------------------ backprojection
 // radon_inversion/backprojection/C/src/integral.c:6-24, output order
 // [iz][ix][iy] at cell centres (radon3d_ajoint.c:240-254):

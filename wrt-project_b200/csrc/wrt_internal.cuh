@@ -187,6 +187,22 @@ int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir
 int staged_scratch(wrt_ctx *ctx, size_t req_bytes);
 void staged_release(wrt_ctx *ctx);
 
+// Ray kernels (k_ray.cu).
+struct RayJob {
+  const float *vol;
+  int n;
+  int nslices, nshift, nphi;
+  const double *trig;   // [nphi][4]: cos phi, sin phi, cos(phi+pi/2), sin(phi+pi/2)
+  const double *shift;  // [nshift]
+  double frame[9];      // row-major rotation of the sample points (has_frame)
+  int has_frame;        // 0: the reference's z-slices
+  const unsigned int *r2bits;
+  double margin;
+  double *out;          // [nslices][nshift][nphi]
+  const float2 *pairs;  // layer pairs [n-1][n][pitch] of the volume, or null
+  int pitch;
+  unsigned long long *counter;  // optional: samples evaluated
+};
 // Batches (batch.cu): many requests in one launch of a captured CUDA graph.
 // The batch is one table in device memory (layout BatchLayout), uploaded by
 // the graph's first node from a pinned host mirror; every kernel of the graph
@@ -211,15 +227,29 @@ struct AdjReq {                    // one backprojection
   const double4 *h_dirw;           // host copy of dirw (launch parameters)
   int ndir, ntheta, nshift, n;
 };
+constexpr int kBatchMaxRay = 64;   // ray-transform requests per batch
+constexpr int kBatchMaxRed = 64;   // reduction requests per batch
+struct RedReq {                    // one ray-to-Radon reduction
+  const double *rays;              // [iz][is][iphi]
+  const double *coef;              // spline elimination coefficients: cp[ns_ray], den[ns_ray]
+  double *scratch;                 // [ngrid*nphi][ns_ray]
+  float4 *lines;                   // [ngrid*nphi][ns_ray - 1]
+  const double *shift;             // [nshift]
+  const double *cs;                // [ntheta][2]: cos, sin theta
+  double *out;                     // [is][iphi][itheta]
+  int ngrid, ns_ray, nphi, nshift, ntheta, pad;
+};
 struct BatchHeader {
-  int nfwd, nadj, nitems, pad;
+  int nfwd, nadj, nitems, nray, nred, pad[3];
 };
 constexpr size_t batch_align(size_t x) { return (x + 255) & ~(size_t)255; }
 struct BatchLayout {
   static constexpr size_t fwd = 256;
   static constexpr size_t aux = batch_align(fwd + sizeof(StagedReq) * kBatchMaxFwd);
   static constexpr size_t adj = batch_align(aux + sizeof(FwdAux) * kBatchMaxFwd);
-  static constexpr size_t items = batch_align(adj + sizeof(AdjReq) * kBatchMaxAdj);
+  static constexpr size_t ray = batch_align(adj + sizeof(AdjReq) * kBatchMaxAdj);
+  static constexpr size_t red = batch_align(ray + sizeof(RayJob) * kBatchMaxRay);
+  static constexpr size_t items = batch_align(red + sizeof(RedReq) * kBatchMaxRed);
   static size_t bytes(size_t nitems) { return items + sizeof(StagedItem) * nitems; }
 };
 // Host-side description of one batch.
@@ -227,11 +257,15 @@ struct BatchBuilder {
   std::vector<StagedReq> fwd;
   std::vector<FwdAux> aux;
   std::vector<AdjReq> adj;
+  std::vector<RayJob> ray;
+  std::vector<RedReq> red;
   std::vector<std::pair<double, StagedItem>> items;  // cost, item
   void clear() {
     fwd.clear();
     aux.clear();
     adj.clear();
+    ray.clear();
+    red.clear();
     items.clear();
   }
 };
@@ -263,23 +297,18 @@ void staged_request(int n, int pitch, int ndir, int nshift, int L, int storage,
                     const void *pairs, const void *vol, const double *dir, const float *dir32,
                     const double *shift, const float *shift32, double *out, StagedReq *r);
 
-// Ray kernels (k_ray.cu).
-struct RayJob {
-  const float *vol;
-  int n;
-  int nslices, nshift, nphi;
-  const double *trig;   // [nphi][4]: cos phi, sin phi, cos(phi+pi/2), sin(phi+pi/2)
-  const double *shift;  // [nshift]
-  double frame[9];      // row-major rotation of the sample points (has_frame)
-  int has_frame;        // 0: the reference's z-slices
-  const unsigned int *r2bits;
-  double margin;
-  double *out;          // [nslices][nshift][nphi]
-  const float2 *pairs;  // layer pairs [n-1][n][pitch] of the volume, or null
-  int pitch;
-  unsigned long long *counter;  // optional: samples evaluated
-};
 int ray_forward(wrt_ctx *ctx, const RayJob &job);
+// Host tables of a ray job (ray_grid/src/init.c:163-176, integral.c:16-24):
+// tab[0..nshift) the shifts, then [nphi][4] cos phi, sin phi, cos(phi+pi/2),
+// sin(phi+pi/2).
+void ray_tables(int nshift, int nphi, double *tab);
+// True when a 3x3 frame is the identity (the reference's z-slices).
+bool identity_frame(const double *frame);
+// Reach of the trilinear sampler around a lattice point (one cell diagonal).
+double trilinear_margin(int n);
+// Line-independent elimination coefficients of the natural cubic spline on
+// ns uniform knots: cp[ns], den[ns].
+void spline_coefficients(int ns, double *cp, double *den);
 
 // Allocation-free backprojection (k_noalloc.cu): drops the cached device
 // address of its working array on a device (a new context may follow a reset).
