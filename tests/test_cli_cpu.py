@@ -56,3 +56,17 @@ def test_reduction_small_flag_takes_no_argument(tmp_path):
     (tmp_path / "r.txt").write_text("0.0\n" * 3)
     r = run("radon_reduction", "-p", "p.txt", "-i", "r.txt", "-s", "-o", "o.txt", cwd=tmp_path)
     assert r.returncode == 1 and "small format" in r.stdout and "end of file" in r.stderr
+
+
+def test_parallel_text_reader(tmp_path):
+    """The programs' chunked multi-threaded reader gives exactly the serial
+    parse's values, takes the first `count` records, and refuses truncated and
+    malformed files (tests/reader_check.c, compiled against cli_common.c)."""
+    cli = PKG_DIR / "cli"
+    exe = tmp_path / "reader_check"
+    subprocess.run(["gcc", "-O2", "-std=gnu99", f"-I{cli}", f"-I{PKG_DIR.parent / 'include'}",
+                    str(Path(__file__).parent / "reader_check.c"), str(cli / "cli_common.c"),
+                    "-o", str(exe), f"-L{PKG_DIR / 'lib'}", "-lwrt", "-lpthread", "-lm",
+                    f"-Wl,-rpath,{PKG_DIR / 'lib'}"], check=True)
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr

@@ -136,48 +136,118 @@ static char *slurp(const char *path, size_t *len) {
   return buf;
 }
 
-static int parse_values(const char *path, size_t count, double *out, int columns) {
-  size_t len = 0;
-  char *buf = slurp(path, &len);
-  if (!buf) return -1;
-  char *p = buf;
-  for (size_t k = 0; k < count; ++k) {
+/* One chunk of the input text, [p, end), parsed on its own thread: every
+ * record (one value, or the 4th of four comma-separated values) into a
+ * growable array.  err: 0, 1 (matching failure at record `bad`), 2 (no memory). */
+typedef struct {
+  const char *p, *end;
+  int columns;
+  double *vals;
+  size_t n, cap, bad;
+  int err;
+} parse_job;
+
+static void *parse_worker(void *arg) {
+  parse_job *j = arg;
+  const char *p = j->p;
+  while (p < j->end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')) ++p;
+  while (p < j->end) {
     double v = 0;
-    for (int c = 0; c < columns; ++c) {
-      char *end;
-      v = strtod(p, &end);
-      if (end == p) {
-        fprintf(stderr,
-                *p ? "Error: %s: matching failure at value %zu, expected %d floating-point value(s).\n"
-                   : "Error: %s: reached the end of file before it was expected (value %zu of %d-column data).\n",
-                path, k, columns);
-        free(buf);
-        return -1;
+    for (int c = 0; c < j->columns; ++c) {
+      char *stop;
+      v = strtod(p, &stop);
+      if (stop == p || stop > j->end) {
+        j->err = 1;
+        j->bad = j->n;
+        return NULL;
       }
-      p = end;
+      p = stop;
       while (*p == ' ' || *p == '\t') ++p;
-      if (c + 1 < columns) {
+      if (c + 1 < j->columns) {
         if (*p != ',') {
-          fprintf(stderr, "Error: %s: matching failure at line %zu, expected %d columns.\n", path, k, columns);
-          free(buf);
-          return -1;
+          j->err = 1;
+          j->bad = j->n;
+          return NULL;
         }
         ++p;
       }
     }
-    out[k] = v;
-    while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n') ++p;
+    if (j->n == j->cap) {
+      size_t cap = j->cap ? 2 * j->cap : 1 << 16;
+      double *nv = realloc(j->vals, cap * sizeof(double));
+      if (!nv) {
+        j->err = 2;
+        return NULL;
+      }
+      j->vals = nv;
+      j->cap = cap;
+    }
+    j->vals[j->n++] = v;
+    while (p < j->end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')) ++p;
   }
+  return NULL;
+}
+
+/* The first `count` records of the file: the text is cut into nthreads
+ * chunks at line ends, parsed in parallel, and the records are taken in file
+ * order (the reference's reader is a serial "%lf" loop, init.c:107-139; same
+ * values, same error cases). */
+static int parse_values(const char *path, size_t count, double *out, int columns, int nthreads) {
+  size_t len = 0;
+  char *buf = slurp(path, &len);
+  if (!buf) return -1;
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > 256) nthreads = 256;
+  if (len < ((size_t)1 << 20)) nthreads = 1;
+  parse_job jobs[256];
+  pthread_t th[256];
+  const char *cut = buf;
+  for (int t = 0; t < nthreads; ++t) {
+    const char *e = t + 1 == nthreads ? buf + len : buf + len / nthreads * (t + 1);
+    if (e < cut) e = cut;
+    while (e < buf + len && *e != '\n') ++e;  /* chunks end at a line end */
+    jobs[t] = (parse_job){cut, e, columns, NULL, 0, 0, 0, 0};
+    cut = e;
+  }
+  for (int t = 0; t < nthreads; ++t)
+    if (nthreads == 1 || pthread_create(&th[t], NULL, parse_worker, &jobs[t]) != 0) {
+      parse_worker(&jobs[t]);
+      th[t] = 0;
+    }
+  for (int t = 0; t < nthreads; ++t)
+    if (nthreads > 1 && th[t]) pthread_join(th[t], NULL);
+  int rc = 0;
+  size_t k = 0;
+  for (int t = 0; t < nthreads && k < count && !rc; ++t) {
+    size_t take = jobs[t].n < count - k ? jobs[t].n : count - k;
+    memcpy(out + k, jobs[t].vals, take * sizeof(double));
+    k += take;
+    if (jobs[t].err == 1 && k < count) {
+      fprintf(stderr, "Error: %s: matching failure at value %zu, expected %d floating-point value(s).\n",
+              path, k, columns);
+      rc = -1;
+    } else if (jobs[t].err == 2) {
+      fprintf(stderr, "Error: %s: out of memory while reading\n", path);
+      rc = -1;
+    }
+  }
+  if (!rc && k < count) {
+    fprintf(stderr,
+            "Error: %s: reached the end of file before it was expected (value %zu of %d-column data).\n",
+            path, k, columns);
+    rc = -1;
+  }
+  for (int t = 0; t < nthreads; ++t) free(jobs[t].vals);
   free(buf);
-  return 0;
+  return rc;
 }
 
-int cli_read_column(const char *path, size_t count, double *out) {
-  return parse_values(path, count, out, 1);
+int cli_read_column(const char *path, size_t count, double *out, int nthreads) {
+  return parse_values(path, count, out, 1, nthreads);
 }
 
-int cli_read_csv4(const char *path, size_t count, double *out) {
-  return parse_values(path, count, out, 4);
+int cli_read_csv4(const char *path, size_t count, double *out, int nthreads) {
+  return parse_values(path, count, out, 4, nthreads);
 }
 
 typedef struct {

@@ -33,10 +33,10 @@ void cli_parse(int argc, char **argv, cli_args *a, const char *usage, int allow_
                int allow_sampler);
 /* Four integers from a parameter file; returns 0 or -1 (message printed). */
 int cli_read_params(const char *path, int p[4]);
-/* count doubles, one per line ("%lf\n"); 0 or -1. */
-int cli_read_column(const char *path, size_t count, double *out);
+/* count doubles, one per line ("%lf\n"), parsed by nthreads threads; 0 or -1. */
+int cli_read_column(const char *path, size_t count, double *out, int nthreads);
 /* count lines "%lf, %lf, %lf, %lf"; keeps the 4th column; 0 or -1. */
-int cli_read_csv4(const char *path, size_t count, double *out);
+int cli_read_csv4(const char *path, size_t count, double *out, int nthreads);
 /* Formats rows with `fmt_row(buf, index, ctx)` in parallel chunks and writes
  * them in order; returns 0 or -1. */
 typedef int (*cli_row_fn)(char *buf, size_t index, const void *ctx);

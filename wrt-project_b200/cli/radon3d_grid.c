@@ -39,7 +39,7 @@ int main(int argc, char **argv) {
     return EXIT_FAILURE;
   }
   printf("  Reading Radon transforms...");
-  if (cli_read_csv4(a.input, nin, radon)) {
+  if (cli_read_csv4(a.input, nin, radon, a.nthreads)) {
     fprintf(stderr, "Aborting : radon_values_init.\n");
     return EXIT_FAILURE;
   }

@@ -40,7 +40,7 @@ int main(int argc, char **argv) {
     return EXIT_FAILURE;
   }
   printf("  Initializing data for ray transforms...");
-  if ((a.small_format ? cli_read_column : cli_read_csv4)(a.input, nin, rays)) {
+  if ((a.small_format ? cli_read_column : cli_read_csv4)(a.input, nin, rays, a.nthreads)) {
     fprintf(stderr, "Aborting : ray_values_init.\n");
     return EXIT_FAILURE;
   }

@@ -48,7 +48,7 @@ int main(int argc, char **argv) {
     return EXIT_FAILURE;
   }
   printf("  Initializing test-function data...");
-  if (cli_read_column(a.input, nvox, vol)) {
+  if (cli_read_column(a.input, nvox, vol, a.nthreads)) {
     fprintf(stderr, "Aborting : tfunction_values_init.\n");
     return EXIT_FAILURE;
   }
