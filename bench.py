@@ -539,6 +539,77 @@ def serving_mix(wrt, dev, count, seed, budget):
             "mean_batch": float(np.mean([i.batch_size for _, i in infos]))}
 
 
+def cli_compare(args):
+    """The drop-in programs against the reference's own programs
+    (oracle/_ref, compiled from its sources), end to end on the same text
+    files, each given all host cores with -n: radon_grid on a 128^3 volume
+    file (2,097,152 lines; 32 longitudes x 16 latitudes x 64 shifts, the
+    reference's default nearest sampler and 4n x 4n lattice), then
+    radon3d_grid of that Radon file back to 64^3.  Wall time per program run
+    (start-up, text input, transform, text output), the programs' own
+    transform times, and the relative L2 difference of the outputs."""
+    import subprocess
+    import tempfile
+
+    from wrt_b200.phantom import ellipsoid_phantom
+
+    sys.path.insert(0, str(ROOT))
+    import oracle as O
+
+    cores = cpu_threads()
+    ours, ref = PKG_DIR / "bin", ROOT / "oracle" / "_ref"
+    if not (ref / "radon_grid").exists():
+        print(json.dumps({"path": "cli", "unavailable": "oracle/_ref programs not built"}))
+        return 0
+    n, nphi, ntheta, nshift, n_adj = N, 32, 16, 64, 64
+    work = Path(tempfile.mkdtemp(prefix="wrt_cli_"))
+    vol = ellipsoid_phantom(n, ELLIPSOIDS, SEED)
+    np.savetxt(work / "volume.txt", vol.reshape(-1), fmt="%lf")
+    (work / "radon_params.txt").write_text(
+        f"{nphi} nphi\n{ntheta} ntheta\n{nshift} nshift\n{n} ngrid\n")
+    (work / "adjoint_params.txt").write_text(
+        f"{nphi} nphi\n{ntheta} ntheta\n{nshift} nshift\n{n_adj} ngrid\n")
+    res = {}
+    for who, bindir in (("ours", ours), ("reference", ref)):
+        d = work / who
+        d.mkdir()
+        row = {}
+        for prog, params, inp, out in (("radon_grid", "radon_params.txt", "../volume.txt",
+                                        "radon.csv"),
+                                       ("radon3d_grid", "adjoint_params.txt", "radon.csv",
+                                        "adjoint.txt")):
+            cmd = [str(bindir / prog), "-p", f"../{params}", "-i", inp, "-o", out, "-n",
+                   str(cores)]
+            t0 = time.perf_counter()
+            r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=1800)
+            wall = time.perf_counter() - t0
+            if r.returncode:
+                raise RuntimeError(f"{who} {prog} failed: {r.stderr[-500:]}")
+            stamp = [ln.strip() for ln in r.stdout.splitlines() if "elapsed" in ln.lower()]
+            row[prog] = {"wall_s": wall, "program_reports": stamp}
+        res[who] = row
+    a = np.loadtxt(work / "ours" / "radon.csv", delimiter=",")[:, 3]
+    b = np.loadtxt(work / "reference" / "radon.csv", delimiter=",")[:, 3]
+    c = np.loadtxt(work / "ours" / "adjoint.txt")
+    d = np.loadtxt(work / "reference" / "adjoint.txt")
+    line = {
+        "path": "cli", "metric": "drop-in program wall time vs the reference's programs",
+        "unit": "s", "higher_is_better": False, "cores": cores,
+        "config": {"radon_grid": f"{n}^3 volume text file, {nphi}x{ntheta} directions x {nshift} "
+                                 "shifts, nearest sampler, 4n x 4n lattice (the defaults)",
+                   "radon3d_grid": f"that Radon file back to {n_adj}^3"},
+        "ours": res["ours"], "reference": res["reference"],
+        "speedup": {p: res["reference"][p]["wall_s"] / res["ours"][p]["wall_s"]
+                    for p in res["ours"]},
+        "rel_l2_outputs": {"radon_grid": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                           "radon3d_grid": float(np.linalg.norm(c - d) / np.linalg.norm(d))},
+        "note": "the reference's text values carry 6 decimals (%lf), so the comparison is "
+                "limited by the printed precision",
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def serving_stream(args, dist):
     """The serving configuration at its stated size: `--requests` (10,000)
     transform requests arriving as a seeded Poisson stream, each a volume of
@@ -1005,7 +1076,7 @@ def main():
                     help="use this tile configuration of the staged kernel instead of tuning")
     ap.add_argument("--requests", type=int, default=10000,
                     help="--path serving: requests in the Poisson stream")
-    ap.add_argument("--path", choices=["forward", "serving", *PATHS], default="forward",
+    ap.add_argument("--path", choices=["forward", "serving", "cli", *PATHS], default="forward",
                     help="forward: the headline (plane integrals at 128^3); ray, reduction, "
                          "adjoint: the other hot paths through their drop-in entry points")
     ap.add_argument("--grid", default=None,
@@ -1018,6 +1089,8 @@ def main():
     try:
         if args.path == "serving":
             rc = serving_stream(args, dist) if args.impl == "ours" and dist.rank == 0 else 0
+        elif args.path == "cli":
+            rc = cli_compare(args) if args.impl == "ours" and dist.rank == 0 else 0
         elif args.path != "forward":
             rc = run_path(args, dist) if args.impl == "ours" else 0
         else:
