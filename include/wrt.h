@@ -155,6 +155,19 @@ int wrt_radon3d_adjoint_static(wrt_ctx *ctx, const double *d_radon, int nphi, in
 int wrt_radon_transpose(wrt_ctx *ctx, const double *g, int ngrid, int nphi, int ntheta,
                         int nshift, const wrt_plane_opts *opts, double *out_volume);
 
+/* Spectral Laplacian of an n^3 volume (any axis order, row-major) sampled on
+ * a periodic cell of length `period` per axis: out = ifftn(U * fftn(in)),
+ * U = -(2 pi / period)^2 (k1^2 + k2^2 + k3^2), k the FFT-order frequencies
+ * (i for i <= n/2, i - n above); the result is real.  The step after the
+ * backprojection in the reference's inversion (f = -1/(8 pi^2) * Laplacian of
+ * the backprojection), radon_inversion/backprojection/laplace3dfft.m:1-25.
+ * Host arrays in and out; FP64 FFTs on the device. */
+int wrt_spectral_laplacian(wrt_ctx *ctx, const double *in, int n, double period, double *out);
+/* The same on device buffers of n^3 doubles, asynchronous on the context's
+ * stream (FFT plans and the spectrum live in the context). */
+int wrt_spectral_laplacian_device(wrt_ctx *ctx, const double *dev_in, int n, double period,
+                                  double *dev_out);
+
 /* ------------------------------------------------ device-resident objects */
 typedef enum wrt_storage {
   WRT_STORAGE_F32 = 0, /* FP32 node values (default) */

@@ -196,6 +196,18 @@ def radon_transpose(g, n, sampler=TRILINEAR, half_extent=None):
     return out
 
 
+def spectral_laplacian(u, period=2.0):
+    """radon_inversion/backprojection/laplace3dfft.m:1-25 in numpy: the real part
+    of ifftn(U * fftn(u)), U = -(2 pi / period)^2 (k1^2 + k2^2 + k3^2) with the
+    FFT-order frequencies k = i (i <= n/2) or i - n (laplace3dfft.m:9-15)."""
+    u = _f64(u)
+    n = u.shape[0]
+    k = np.array([i if i <= n // 2 else i - n for i in range(n)], dtype=np.float64)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
+    U = -(2.0 * np.pi / period) ** 2 * k2
+    return np.real(np.fft.ifftn(U * np.fft.fftn(u)))
+
+
 # ------------------------------------------------- the reference, compiled here
 class Reference:
     """The reference's own hot-path code (oracle/_ref), via small drivers."""

@@ -153,3 +153,24 @@ def test_spline_and_quadratic_reproduce_their_spaces():
     rays[-1] = 0  # values beyond iz >= ngrid-2 are taken as 0 by the reference; avoid that band
     out = O.reduction_forward(rays, ns, nth)
     assert np.isfinite(out).all()
+
+
+def test_spectral_laplacian_restatement_on_eigenfunctions():
+    """The numpy restatement of laplace3dfft.m (the reference's Octave script
+    cannot run here) is pinned by closed forms: on the periodic cell [-1, 1)
+    (period 2) a product of sines and cosines with integer frequencies below
+    n/2 is an eigenfunction, Laplacian = -(2 pi / period)^2 (a^2 + b^2 + c^2) u;
+    constants map to zero; the operator is linear and symmetric."""
+    for n in (16, 21, 32):
+        c = -1.0 + (2.0 * np.arange(n) + 1.0) / n
+        X, Y, Z = np.meshgrid(c, c, c, indexing="ij")
+        for a, b, d in ((1, 0, 0), (3, 2, 5), (n // 2 - 1, 1, 2)):
+            u = np.sin(np.pi * a * X) * np.cos(np.pi * b * Y) * np.sin(np.pi * d * Z)
+            lap = O.spectral_laplacian(u, 2.0)
+            assert np.abs(lap + np.pi ** 2 * (a * a + b * b + d * d) * u).max() < 1e-9 * (a * a + b * b + d * d + 1)
+        assert np.abs(O.spectral_laplacian(np.full((n, n, n), 3.0), 2.0)).max() < 1e-12
+        rng = np.random.default_rng(n)
+        f, g = rng.standard_normal((2, n, n, n))
+        assert np.allclose(O.spectral_laplacian(2 * f - g), 2 * O.spectral_laplacian(f)
+                           - O.spectral_laplacian(g), atol=1e-9)
+        assert abs((O.spectral_laplacian(f) * g).sum() - (f * O.spectral_laplacian(g)).sum()) < 1e-7 * n ** 3

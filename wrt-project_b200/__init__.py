@@ -122,6 +122,8 @@ def lib() -> C.CDLL:
         L.wrt_radon_reduction.argtypes = [_vp, _dp, _i, _i, _i, _i, _i, _dp]
         L.wrt_radon3d_adjoint.argtypes = [_vp, _dp, _i, _i, _i, _i, _dp]
         L.wrt_radon_transpose.argtypes = [_vp, _dp, _i, _i, _i, _i, C.POINTER(PlaneOpts), _dp]
+        L.wrt_spectral_laplacian.argtypes = [_vp, _dp, _i, C.c_double, _dp]
+        L.wrt_spectral_laplacian_device.argtypes = [_vp, _vp, _i, C.c_double, _vp]
         L.wrt_volume_create.argtypes = [_vp, _i, C.POINTER(_vp)]
         L.wrt_volume_create_storage.argtypes = [_vp, _i, _i, C.POINTER(_vp)]
         L.wrt_volume_bytes.argtypes = [_vp]
@@ -301,6 +303,24 @@ class Context:
         self.check(lib().wrt_radon3d_adjoint(self._h, R, nphi, ntheta, nshift, ngrid, out),
                    "radon3d_adjoint")
         return out
+
+    def spectral_laplacian(self, volume, period=2.0) -> np.ndarray:
+        """ifftn(-(2 pi/period)^2 |k|^2 fftn(volume)) of an n^3 array
+        (laplace3dfft.m), FP64 FFTs on the device."""
+        v = _f64(volume)
+        n = v.shape[0]
+        assert v.shape == (n, n, n)
+        out = np.empty_like(v)
+        self.check(lib().wrt_spectral_laplacian(self._h, v, n, float(period), out),
+                   "spectral_laplacian")
+        return out
+
+    def backprojection_inversion(self, radon, ngrid) -> np.ndarray:
+        """The reference's backprojection inversion of Radon data on the
+        Gauss-uniform sphere grid: f = -1/(8 pi^2) * Laplacian of the
+        backprojection (cell-centred ngrid^3 grid on [-1, 1]^3, [iz][ix][iy])."""
+        return self.spectral_laplacian(self.radon3d_adjoint(radon, ngrid), 2.0) * (
+            -1.0 / (8.0 * np.pi ** 2))
 
     def radon_transpose(self, g, ngrid, sampler=TRILINEAR, half_extent=0) -> np.ndarray:
         g = _f64(g)

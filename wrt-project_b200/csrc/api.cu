@@ -268,6 +268,7 @@ int wrt_ctx_destroy(wrt_ctx *ctx) {
   staged_release(ctx);
   if (ctx->dropin_vol) wrt_volume_destroy(ctx->dropin_vol);
   if (ctx->dropin_grid) wrt_grid_destroy(ctx->dropin_grid);
+  laplace_release(ctx);
   for (int r = 0; r < WS_ROLES; ++r) ctx_free(ctx, ctx->ws[r], ctx->ws_bytes[r]);
   cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -60,6 +60,7 @@ struct wrt_ctx {
   // context: warm calls of the same or smaller sizes allocate nothing
   void *ws[8] = {};
   size_t ws_bytes[8] = {};
+  void *fft_plans = nullptr;  // spectral Laplacian plans (k_laplace.cu)
   // the volume and sphere grid of the last drop-in (host-array) call, kept
   // for the next call of the same sizes
   wrt_volume *dropin_vol = nullptr;
@@ -76,7 +77,7 @@ void ctx_free(wrt_ctx *ctx, void *p, size_t bytes);
 int check_launch(wrt_ctx *ctx, const char *what);
 // Working buffer of a role, at least `bytes` long (grown after the context's
 // stream has drained; contents are not kept).
-enum WsRole { WS_STAGE, WS_IN, WS_OUT, WS_LINES, WS_SPLINE, WS_COEF, WS_TABLE, WS_ROLES };
+enum WsRole { WS_STAGE, WS_IN, WS_OUT, WS_LINES, WS_SPLINE, WS_COEF, WS_TABLE, WS_FFT, WS_ROLES };
 int ws_get(wrt_ctx *ctx, int role, size_t bytes, void **p);
 
 // Host-side FP64 geometry, computed with the host libm exactly as the
@@ -309,6 +310,11 @@ double trilinear_margin(int n);
 // Line-independent elimination coefficients of the natural cubic spline on
 // ns uniform knots: cp[ns], den[ns].
 void spline_coefficients(int ns, double *cp, double *den);
+
+// Spectral Laplacian (k_laplace.cu) of an n^3 device volume into d_out, and
+// the release of the context's FFT plans.
+int spectral_laplacian(wrt_ctx *ctx, const double *d_in, int n, double period, double *d_out);
+void laplace_release(wrt_ctx *ctx);
 
 // Allocation-free backprojection (k_noalloc.cu): drops the cached device
 // address of its working array on a device (a new context may follow a reset).
