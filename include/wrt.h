@@ -168,6 +168,41 @@ int wrt_spectral_laplacian(wrt_ctx *ctx, const double *in, int n, double period,
 int wrt_spectral_laplacian_device(wrt_ctx *ctx, const double *dev_in, int n, double period,
                                   double *dev_out);
 
+/* ------------------------------------------- analytic test functions */
+/* The reference's analytic-function programs (radon_analytic, ray_analytic)
+ * integrate a function compiled into the binary; its two example files are
+ * the families below, with their constants as parameters here. */
+typedef enum wrt_function_kind {
+  /* exp(-1 / (R2 - |x - c|^2)) where |x - c|^2 < R2 - eps, else 0
+   * (radon_analytic/examples-test-functions/exponential_bump.c: c = (0.2, 0, 0),
+   * R2 = 0.5, eps = 1e-2); p = {cx, cy, cz, R2, eps} */
+  WRT_FUNCTION_EXP_BUMP = 0,
+  /* sum of `count` balls, each amplitude inside rin, a sine transition
+   * amplitude/(20 pi) (-sin 6t/3 + 3 sin 4t - 15 sin 2t + 20 t), t = pi (r - rout)/
+   * (rout - rin), between rin and rout, 0 beyond (.../sinusoidal_bump.c);
+   * p = {cx, cy, cz, amplitude, rin, rout} per ball */
+  WRT_FUNCTION_SINE_BUMPS = 1
+} wrt_function_kind;
+#define WRT_FUNCTION_MAX_BALLS 8
+typedef struct wrt_function {
+  int kind;   /* wrt_function_kind */
+  int count;  /* sine bumps: balls, 1..WRT_FUNCTION_MAX_BALLS */
+  double p[6 * WRT_FUNCTION_MAX_BALLS];
+} wrt_function;
+
+/* radon_analytic: out[is][iphi][itheta] = plane integral of f over the
+ * reference's lattice (radon_analytic/src/integral.c:25-57: points
+ * s n + delta (i v1 + j v2), i, j in [-2n, 2n), delta = 1/(n - 1), weight
+ * delta^2) on the Gauss-uniform sphere grid; loop nest
+ * radon_analytic/src/radon_analytic.c:244-262. */
+int wrt_radon_analytic(wrt_ctx *ctx, const wrt_function *f, int ngrid, int nphi, int ntheta,
+                       int nshift, double *out);
+/* ray_analytic: out[iz][is][iphi] = ray integral of f on z-slice
+ * z = -1 + 2 iz/(n - 1), iz < n (ray_analytic/integral.c:10-48, loop nest
+ * ray_analytic/ray_analytic.c:254-272). */
+int wrt_ray_analytic(wrt_ctx *ctx, const wrt_function *f, int ngrid, int nshift, int nphi,
+                     double *out);
+
 /* ------------------------------------------------ device-resident objects */
 typedef enum wrt_storage {
   WRT_STORAGE_F32 = 0, /* FP32 node values (default) */

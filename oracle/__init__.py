@@ -231,6 +231,41 @@ class Reference:
     def available() -> bool:
         return (HERE / "_ref" / "libref_radon_grid.so").exists()
 
+    @staticmethod
+    def analytic(kind: str, family: str):
+        """The reference's radon_analytic ('plane') or ray_analytic ('ray')
+        integrator compiled with its example function `family` ('exp':
+        exponential_bump.c, 'sine': sinusoidal_bump.c)."""
+        name = {"plane": "radon_analytic", "ray": "ray_analytic"}[kind]
+        L = _load(HERE / "_ref" / f"libref_{name}_{family}.so")
+        if kind == "plane":
+            L.refdrv_analytic_planes.argtypes = [_i, _i, _dp, _dp, _dp, _dp, _i]
+        else:
+            L.refdrv_analytic_rays.argtypes = [_i, _i, _dp, _dp, _dp, _dp, _i]
+        L.refdrv_analytic_values.argtypes = [_i, _dp, _dp, _dp, _dp]
+        return L
+
+    def analytic_planes(self, family, ngrid, phi, theta, shift, nthreads=None):
+        L = self.analytic("plane", family)
+        phi, theta, shift = _f64(phi), _f64(theta), _f64(shift)
+        out = np.empty(phi.shape[0])
+        L.refdrv_analytic_planes(ngrid, phi.shape[0], phi, theta, shift, out, _nthreads(nthreads))
+        return out
+
+    def analytic_rays(self, family, ngrid, z, shift, phi, nthreads=None):
+        L = self.analytic("ray", family)
+        z, shift, phi = _f64(z), _f64(shift), _f64(phi)
+        out = np.empty(z.shape[0])
+        L.refdrv_analytic_rays(ngrid, z.shape[0], z, shift, phi, out, _nthreads(nthreads))
+        return out
+
+    def analytic_values(self, family, x, y, z):
+        L = self.analytic("plane", family)
+        x, y, z = _f64(x), _f64(y), _f64(z)
+        out = np.empty(x.shape[0])
+        L.refdrv_analytic_values(x.shape[0], x, y, z, out)
+        return out
+
     def radon_grid(self, nphi, ntheta, nshift):
         phi, th, s = np.empty(nphi), np.empty(ntheta), np.empty(nshift)
         self.radon.refdrv_radon_grid_init(nphi, ntheta, nshift, phi, th, s)

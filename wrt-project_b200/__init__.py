@@ -55,6 +55,35 @@ class ForwardReq(C.Structure):
 
 
 OP_FORWARD, OP_ADJOINT, OP_RAY, OP_REDUCE = 0, 1, 2, 3
+FUNCTION_EXP_BUMP, FUNCTION_SINE_BUMPS = 0, 1
+
+
+class Function(C.Structure):
+    """An analytic test function (wrt_function): FUNCTION_EXP_BUMP with
+    p = (cx, cy, cz, R2, eps), or FUNCTION_SINE_BUMPS with p = (cx, cy, cz,
+    amplitude, rin, rout) per ball."""
+    _fields_ = [("kind", C.c_int), ("count", C.c_int), ("p", C.c_double * 48)]
+
+
+def exp_bump(center=(0.2, 0.0, 0.0), R2=0.5, eps=1e-2) -> Function:
+    """The reference's exponential_bump.c (its constants by default)."""
+    f = Function()
+    f.kind, f.count = FUNCTION_EXP_BUMP, 1
+    for k, v in enumerate([*center, R2, eps]):
+        f.p[k] = v
+    return f
+
+
+def sine_bumps(balls=((0.0, 0.2, 0.0, 1.0, 0.4, 0.6), (-0.5, 0.0, 0.0, 0.6, 0.3, 0.45),
+                      (0.0, 0.2, 0.5, 0.3, 0.4, 0.6))) -> Function:
+    """The reference's sinusoidal_bump.c (its three balls by default):
+    each ball (cx, cy, cz, amplitude, rin, rout)."""
+    f = Function()
+    f.kind, f.count = FUNCTION_SINE_BUMPS, len(balls)
+    for b, ball in enumerate(balls):
+        for k, v in enumerate(ball):
+            f.p[6 * b + k] = v
+    return f
 
 
 class Request(C.Structure):
@@ -123,6 +152,8 @@ def lib() -> C.CDLL:
         L.wrt_radon3d_adjoint.argtypes = [_vp, _dp, _i, _i, _i, _i, _dp]
         L.wrt_radon_transpose.argtypes = [_vp, _dp, _i, _i, _i, _i, C.POINTER(PlaneOpts), _dp]
         L.wrt_spectral_laplacian.argtypes = [_vp, _dp, _i, C.c_double, _dp]
+        L.wrt_radon_analytic.argtypes = [_vp, C.POINTER(Function), _i, _i, _i, _i, _dp]
+        L.wrt_ray_analytic.argtypes = [_vp, C.POINTER(Function), _i, _i, _i, _dp]
         L.wrt_spectral_laplacian_device.argtypes = [_vp, _vp, _i, C.c_double, _vp]
         L.wrt_volume_create.argtypes = [_vp, _i, C.POINTER(_vp)]
         L.wrt_volume_create_storage.argtypes = [_vp, _i, _i, C.POINTER(_vp)]
@@ -302,6 +333,21 @@ class Context:
         out = np.empty((ngrid, ngrid, ngrid))
         self.check(lib().wrt_radon3d_adjoint(self._h, R, nphi, ntheta, nshift, ngrid, out),
                    "radon3d_adjoint")
+        return out
+
+    def radon_analytic(self, function, ngrid, nphi, ntheta, nshift) -> np.ndarray:
+        """radon_analytic: plane integrals [s][phi][theta] of an analytic
+        function (Function) on the reference's lattice for grid density ngrid."""
+        out = np.empty((nshift, nphi, ntheta))
+        self.check(lib().wrt_radon_analytic(self._h, C.byref(function), int(ngrid), int(nphi),
+                                            int(ntheta), int(nshift), out), "radon_analytic")
+        return out
+
+    def ray_analytic(self, function, ngrid, nshift, nphi) -> np.ndarray:
+        """ray_analytic: ray integrals [z][s][phi] on ngrid z-slices."""
+        out = np.empty((ngrid, nshift, nphi))
+        self.check(lib().wrt_ray_analytic(self._h, C.byref(function), int(ngrid), int(nshift),
+                                          int(nphi), out), "ray_analytic")
         return out
 
     def spectral_laplacian(self, volume, period=2.0) -> np.ndarray:

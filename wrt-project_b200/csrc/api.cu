@@ -106,6 +106,11 @@ void ray_tables(int nshift, int nphi, double *tab) {
 
 double trilinear_margin(int n) { return sqrt(3.0) * (2.0 / (n - 1)) + 1e-6; }
 
+void grid_tables(const wrt_grid *g, const double **dir, const double **shift) {
+  *dir = g->d_dir;
+  *shift = g->d_shift;
+}
+
 bool identity_frame(const double *f) {
   return !f || (f[0] == 1.0 && f[4] == 1.0 && f[8] == 1.0 && f[1] == 0.0 && f[2] == 0.0 &&
                 f[3] == 0.0 && f[5] == 0.0 && f[6] == 0.0 && f[7] == 0.0);

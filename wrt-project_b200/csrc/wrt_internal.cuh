@@ -303,6 +303,8 @@ int ray_forward(wrt_ctx *ctx, const RayJob &job);
 // tab[0..nshift) the shifts, then [nphi][4] cos phi, sin phi, cos(phi+pi/2),
 // sin(phi+pi/2).
 void ray_tables(int nshift, int nphi, double *tab);
+// Device tables of a grid: FP64 directions [ndir][9] and shifts [nshift].
+void grid_tables(const wrt_grid *g, const double **dir, const double **shift);
 // True when a 3x3 frame is the identity (the reference's z-slices).
 bool identity_frame(const double *frame);
 // Reach of the trilinear sampler around a lattice point (one cell diagonal).
