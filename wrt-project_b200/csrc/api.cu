@@ -30,6 +30,9 @@ struct wrt_volume {
   int storage = WRT_STORAGE_F32;        // BF16: d_vol16 / d_pairs16 replace d_vol / d_pairs
   __nv_bfloat16 *d_vol16 = nullptr;     // n^3 bf16 values, v[ix][iy][iz]
   __nv_bfloat162 *d_pairs16 = nullptr;  // layer pairs as bf16x2
+  float4 *d_oct = nullptr;              // cell octets (ray transforms in rotated frames)
+  size_t oct_bytes = 0;
+  bool oct_valid = false;
 };
 
 struct wrt_grid {
@@ -454,7 +457,22 @@ int volume_finish_upload(wrt_volume *v) {
   memcpy(&v->r2, &stats[0], sizeof(float));
   memcpy(&v->maxabs, &stats[1], sizeof(float));
   v->pairs_valid = false;
+  v->oct_valid = false;
   return WRT_OK;
+}
+
+int volume_ensure_octets(wrt_volume *v) {
+  if (v->oct_valid) return WRT_OK;
+  wrt_ctx *ctx = v->ctx;
+  if (!v->d_oct) {
+    const size_t m = (size_t)(v->n - 1);
+    v->oct_bytes = 2 * sizeof(float4) * m * m * m;
+    int st = ctx_alloc(ctx, (void **)&v->d_oct, v->oct_bytes);
+    if (st) return st;
+  }
+  int st = volume_octets(ctx, v->d_vol, v->n, v->d_oct);
+  if (!st) v->oct_valid = true;
+  return st;
 }
 
 int volume_ensure_pairs(wrt_volume *v) {
@@ -511,7 +529,7 @@ int wrt_volume_upload_device(wrt_volume *v, const float *dev_f32) {
 }
 
 size_t wrt_volume_bytes(const wrt_volume *v) {
-  return v ? v->vol_bytes + v->pair_bytes + 2 * sizeof(unsigned int) : 0;
+  return v ? v->vol_bytes + v->pair_bytes + v->oct_bytes + 2 * sizeof(unsigned int) : 0;
 }
 
 int wrt_volume_destroy(wrt_volume *v) {
@@ -524,6 +542,7 @@ int wrt_volume_destroy(wrt_volume *v) {
   ctx_free(ctx, v->d_stats, 2 * sizeof(unsigned int));
   ctx_free(ctx, v->d_pairs, v->pair_bytes);
   ctx_free(ctx, v->d_pairs16, v->pair_bytes);
+  ctx_free(ctx, v->d_oct, v->oct_bytes);
   delete v;
   return WRT_OK;
 }
@@ -915,8 +934,10 @@ int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const double *f
   st = ws_get(ctx, WS_TABLE, sizeof(double) * tab.size(), &dtab);
   // a copy from pageable memory returns once the data is staged
   if (!st) st = h2d(ctx, dtab, tab.data(), sizeof(double) * tab.size(), "ray grid");
-  // z-slices read one layer pair each: the volume's layer pairs (built once)
+  // z-slices read one layer pair each: the volume's layer pairs (built once);
+  // rotated layers read cell octets (built once)
   if (!st && identity) st = volume_ensure_pairs(vol);
+  if (!st && !identity) st = volume_ensure_octets(vol);
   if (st) return st;
   RayJob job = {};
   job.vol = vol->d_vol;
@@ -936,6 +957,8 @@ int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const double *f
   if (identity) {
     job.pairs = vol->d_pairs;
     job.pitch = vol->pitch;
+  } else {
+    job.oct = vol->d_oct;
   }
   return ray_forward(ctx, job);
 }

@@ -14,7 +14,11 @@
 //              any input, not an assumption about the support.
 //   * d_pairs  layer pairs for the staged plane kernel: pairs[iz][iy][ix] =
 //              (v[ix][iy][iz], v[ix][iy][iz+1]) for iz in [0, n-2], rows
-//              padded to `pitch` elements so every row starts 16-byte aligned.
+//              padded to `pitch` elements so every row starts 16-byte aligned;
+//   * d_oct    cell octets for ray transforms in rotated layer frames: cell
+//              (ix, iy, iz), ix, iy, iz in [0, n-2], holds its eight corners
+//              as two float4, (v(x,y,z), v(x,y,z+1), v(x,y+1,z), v(x,y+1,z+1))
+//              at x = ix and at x = ix + 1, one 32-byte sector per sample.
 #include "wrt_internal.cuh"
 
 namespace {
@@ -42,6 +46,19 @@ __global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *_
   if ((threadIdx.x & 31) == 0) {
     if (local > 0.0f) atomicMax(stats, __float_as_uint(local));
     if (amax > 0.0f) atomicMax(stats + 1, __float_as_uint(amax));
+  }
+}
+
+// oct[2c], oct[2c+1]: corners of cell c = (ix*(n-1) + iy)*(n-1) + iz.
+__global__ void volume_octets_kernel(const float *__restrict__ v, int n, float4 *__restrict__ oct) {
+  const size_t m = (size_t)(n - 1), total = m * m * m;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total;
+       c += (size_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(c % m), iy = (int)((c / m) % m), ix = (int)(c / (m * m));
+    const float *q = v + ((size_t)ix * n + iy) * n + iz;
+    const size_t sx = (size_t)n * n;
+    oct[2 * c] = make_float4(q[0], q[1], q[n], q[n + 1]);
+    oct[2 * c + 1] = make_float4(q[sx], q[sx + 1], q[sx + n], q[sx + n + 1]);
   }
 }
 
@@ -141,6 +158,12 @@ int volume_pairs_bf16(wrt_ctx *ctx, const __nv_bfloat16 *d_vol16, int n,
   volume_pairs_bf16_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(d_vol16, n, d_pairs, pitch);
   ctx->launches++;
   return check_launch(ctx, "volume_pairs_bf16_kernel");
+}
+
+int volume_octets(wrt_ctx *ctx, const float *d_vol, int n, float4 *d_oct) {
+  volume_octets_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(d_vol, n, d_oct);
+  ctx->launches++;
+  return check_launch(ctx, "volume_octets_kernel");
 }
 
 int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch) {

@@ -72,6 +72,24 @@ struct Corners {
   }
 };
 
+// Trilinear at FP32 cell coordinates (outside the guard band, inside
+// [0, n-1]) from the cell octets: two 16-byte loads of one 32-byte sector,
+// then the same FP32 operations in the same order as wrtd::tri32 (x, then y,
+// then z; the x and y steps on packed pairs), so the value is bitwise tri32's.
+__device__ __forceinline__ float tri32_octets(const float4 *__restrict__ oct, int n, float qx,
+                                              float qy, float qz) {
+  const float fx = floorf(qx), fy = floorf(qy), fz = floorf(qz);
+  const float tx = qx - fx, ty = qy - fy, tz = qz - fz;
+  const int m = n - 1;
+  const size_t c = ((size_t)(int)fx * m + (int)fy) * m + (int)fz;
+  const float4 lo = __ldg(oct + 2 * c), hi = __ldg(oct + 2 * c + 1);
+  // (a0, b0) = lerp_x of (v(x,y,z), v(x,y,z+1)); (a1, b1) of the y+1 pair
+  const float a0 = lerp32(tx, lo.x, hi.x), b0 = lerp32(tx, lo.y, hi.y);
+  const float a1 = lerp32(tx, lo.z, hi.z), b1 = lerp32(tx, lo.w, hi.w);
+  const float e0 = lerp32(ty, a0, a1), e1 = lerp32(ty, b0, b1);
+  return lerp32(tz, e0, e1);
+}
+
 // Ray number `ray` (0 <= ray < nslices * nshift * nphi, shift fastest) of a job.
 template <bool FRAME>
 __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, float guard) {
@@ -171,7 +189,7 @@ __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, f
         } else if (qx > 0.0f && qy > 0.0f && qx < qmax && qy < qmax &&
                    (!FRAME || (qz > 0.0f && qz < qmax))) {
           if (FRAME) {
-            part += wrtd::tri32(job.vol, n, qx, qy, qz);
+            part += job.oct ? tri32_octets(job.oct, n, qx, qy, qz) : wrtd::tri32(job.vol, n, qx, qy, qz);
           } else {
             // bilinear in x, y on layers zc and zc+1, then the ray's z weight
             const float fx = floorf(qx), fy = floorf(qy);

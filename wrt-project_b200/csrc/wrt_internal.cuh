@@ -102,6 +102,8 @@ int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
 int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
                     unsigned int *d_stats);
 int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch);
+// Cell octets: 2 (n-1)^3 float4, the eight corners of every cell.
+int volume_octets(wrt_ctx *ctx, const float *d_vol, int n, float4 *d_oct);
 // BF16 storage: values rounded to bfloat16 (nearest even); statistics of the
 // rounded values; layer pairs as bf16x2.
 int volume_to_bf16(wrt_ctx *ctx, const float *d_vol, int n, __nv_bfloat16 *d_vol16,
@@ -123,6 +125,7 @@ struct PlaneJob {
   double margin;         // crop radius = sqrt(r2) + margin (>= the sampler's reach)
   double *out;           // [nshift][ndir]
   unsigned long long *counter;  // optional: samples evaluated
+  const float4 *oct;    // cell octets of the volume (rotated frames), or null
 };
 int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job);
 int plane_transpose(wrt_ctx *ctx, const PlaneJob &job, const double *d_g, double *d_vol64);
@@ -203,6 +206,7 @@ struct RayJob {
   const float2 *pairs;  // layer pairs [n-1][n][pitch] of the volume, or null
   int pitch;
   unsigned long long *counter;  // optional: samples evaluated
+  const float4 *oct;    // cell octets of the volume (rotated frames), or null
 };
 // Batches (batch.cu): many requests in one launch of a captured CUDA graph.
 // The batch is one table in device memory (layout BatchLayout), uploaded by
