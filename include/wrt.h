@@ -168,6 +168,18 @@ int wrt_spectral_laplacian(wrt_ctx *ctx, const double *in, int n, double period,
 int wrt_spectral_laplacian_device(wrt_ctx *ctx, const double *dev_in, int n, double period,
                                   double *dev_out);
 
+/* Inversion of Radon data R[is][iphi][itheta] on the Gauss-uniform sphere
+ * grid (shifts uniform on [-rsupp, rsupp]) through the Fourier slice theorem:
+ * the 1D Fourier transform of every projection along the shift, zero-padded
+ * to padding * floor(1/ds) points (ds = 2 rsupp/(nshift - 1)), and the inverse
+ * 3D Fourier integral in spherical coordinates, 1/2 sum nu^2 dnu dphi w_theta,
+ * evaluated exactly at the ngrid^3 points -1 + 2 l/ngrid of [-1, 1)^3, order
+ * [ix][iy][iz].  The reference's route is radon_inversion/rtft3d.m followed by
+ * nfft_reconstruct_3d.m (an adjoint NFFT); here nodes carry physical
+ * frequencies and the nonuniform sum is exact. */
+int wrt_fourier_slice_inversion(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
+                                int nshift, double rsupp, int padding, int ngrid, double *out);
+
 /* ------------------------------------------- analytic test functions */
 /* The reference's analytic-function programs (radon_analytic, ray_analytic)
  * integrate a function compiled into the binary; its two example files are

@@ -153,6 +153,7 @@ def lib() -> C.CDLL:
         L.wrt_radon_transpose.argtypes = [_vp, _dp, _i, _i, _i, _i, C.POINTER(PlaneOpts), _dp]
         L.wrt_spectral_laplacian.argtypes = [_vp, _dp, _i, C.c_double, _dp]
         L.wrt_radon_analytic.argtypes = [_vp, C.POINTER(Function), _i, _i, _i, _i, _dp]
+        L.wrt_fourier_slice_inversion.argtypes = [_vp, _dp, _i, _i, _i, C.c_double, _i, _i, _dp]
         L.wrt_ray_analytic.argtypes = [_vp, C.POINTER(Function), _i, _i, _i, _dp]
         L.wrt_spectral_laplacian_device.argtypes = [_vp, _vp, _i, C.c_double, _vp]
         L.wrt_volume_create.argtypes = [_vp, _i, C.POINTER(_vp)]
@@ -333,6 +334,18 @@ class Context:
         out = np.empty((ngrid, ngrid, ngrid))
         self.check(lib().wrt_radon3d_adjoint(self._h, R, nphi, ntheta, nshift, ngrid, out),
                    "radon3d_adjoint")
+        return out
+
+    def fourier_slice_inversion(self, radon, ngrid, rsupp=1.0, padding=4) -> np.ndarray:
+        """f on the ngrid^3 points -1 + 2l/ngrid ([ix][iy][iz]) from Radon data
+        [s][phi][theta] via the Fourier slice theorem (rtft3d.m +
+        nfft_reconstruct_3d.m, exact nonuniform sum)."""
+        R = _f64(radon)
+        nshift, nphi, ntheta = R.shape
+        out = np.empty((ngrid, ngrid, ngrid))
+        self.check(lib().wrt_fourier_slice_inversion(self._h, R, nphi, ntheta, nshift,
+                                                     float(rsupp), int(padding), int(ngrid), out),
+                   "fourier_slice_inversion")
         return out
 
     def radon_analytic(self, function, ngrid, nphi, ntheta, nshift) -> np.ndarray:
