@@ -331,7 +331,19 @@ def other_paths(wrt, ctx, phantom, steps, warmup, smem_bw, with_cpu):
     adjoint = entry("adjoint", adj, n ** 3, "voxels/s", 16, evals,
                     "spline evaluation (one 16 B record)",
                     lambda: adj_d.download(np.empty((n, n, n))))
-    for k, w in (("ray", "128^3, 128 layers x 128 shifts x 128 angles, reference frame"),
+    # the reference's default sampler: nearest cell on the 4n x 4n lattice
+    near = lambda: wrt.radon_forward_device(ctx, vol, grid, radon_d.ptr, sampler=wrt.NEAREST)
+    nearest = entry("nearest", near, grid.nplanes, "plane integrals/s", 4, counted(near),
+                    "nearest sample (one FP32 cell value)",
+                    lambda: radon_d.download(np.empty((NSHIFT, NPHI, NTHETA))))
+    plain_near = lambda: wrt.radon_forward_device(ctx, vol, grid, radon_d.ptr, sampler=wrt.NEAREST,
+                                                  kernel=wrt.KERNEL_PLAIN)
+    pt = timed_device_calls(ctx, plain_near, 2, 1)
+    res["nearest"]["plain_kernel_ms"] = statistics.mean(pt)
+    res["nearest"]["over_plain"] = statistics.mean(pt) / res["nearest"]["ms_per_call"]
+    for k, w in (("nearest", "128^3, 64x128 sphere grid x 256 shifts, nearest sampler, lattice "
+                             "[-2n, 2n)^2 with step 1/n (radon_grid's defaults)"),
+                 ("ray", "128^3, 128 layers x 128 shifts x 128 angles, reference frame"),
                  ("ray_rotated", "the same in one seeded rotated layer frame"),
                  ("reduction", "128^3 rays (128 offsets) -> 64x128 sphere grid x 256 shifts"),
                  ("adjoint", "N(0,1) Radon data 64x128x256 -> 128^3 voxels")):
@@ -341,6 +353,22 @@ def other_paths(wrt, ctx, phantom, steps, warmup, smem_bw, with_cpu):
         cores = cpu_threads()
         ref = O.Reference() if O.Reference.available() else None
         s_grid, phi_grid = O.ray_grid(RAY_SHIFTS, RAY_PHIS)
+        # nearest: the reference's own plane_integral (its default sampler) on
+        # 1024 seeded planes
+        if ref:
+            m = 1024
+            idx = rng.integers(0, grid.nplanes, size=m)
+            it, ip, i_s = idx % NTHETA, (idx // NTHETA) % NPHI, idx // (NTHETA * NPHI)
+            phi, theta, _, shift = O.radon_grid(NPHI, NTHETA, NSHIFT)
+            t0 = time.perf_counter()
+            got = ref.plane_integrals(phantom, phi[ip], theta[it], shift[i_s], cores)
+            wall = time.perf_counter() - t0
+            res["nearest"]["cpu_baseline"] = {
+                "value": m / wall, "unit": "plane integrals/s", "cores": cores,
+                "kind": "reference",
+                "sample": f"{m} seeded planes, radon_grid's plane_integral (oracle/_ref), FP64"}
+            res["nearest"]["rel_l2_vs_reference_on_sample"] = float(
+                np.linalg.norm(nearest.reshape(-1)[idx] - got) / np.linalg.norm(got))
         # ray: the reference's ray_transform on 16384 seeded rays
         m = 16384
         idx = rng.integers(0, nrays, size=m)

@@ -58,7 +58,8 @@ typedef enum wrt_sampler {
 } wrt_sampler;
 
 typedef enum wrt_kernel {
-  WRT_KERNEL_AUTO = 0,   /* staged kernel when it applies */
+  WRT_KERNEL_AUTO = 0,   /* trilinear: the staged kernel when it applies; nearest: rows
+                            walked by whole warps over a z-major copy of the volume */
   WRT_KERNEL_PLAIN = 1,  /* one warp per plane, gathers through L1 */
   WRT_KERNEL_STAGED = 2  /* volume layers staged in shared memory, persistent CTAs */
 } wrt_kernel;

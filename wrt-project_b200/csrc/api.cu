@@ -33,6 +33,8 @@ struct wrt_volume {
   float4 *d_oct = nullptr;              // cell octets (ray transforms in rotated frames)
   size_t oct_bytes = 0;
   bool oct_valid = false;
+  float *d_layers = nullptr;            // z-major copy [iz][iy][ix] (nearest sampler)
+  bool layers_valid = false;
 };
 
 struct wrt_grid {
@@ -458,7 +460,19 @@ int volume_finish_upload(wrt_volume *v) {
   memcpy(&v->maxabs, &stats[1], sizeof(float));
   v->pairs_valid = false;
   v->oct_valid = false;
+  v->layers_valid = false;
   return WRT_OK;
+}
+
+int volume_ensure_layers(wrt_volume *v) {
+  if (v->layers_valid) return WRT_OK;
+  if (!v->d_layers) {
+    int st = ctx_alloc(v->ctx, (void **)&v->d_layers, v->vol_bytes);
+    if (st) return st;
+  }
+  int st = volume_layers(v->ctx, v->d_vol, v->n, v->d_layers);
+  if (!st) v->layers_valid = true;
+  return st;
 }
 
 int volume_ensure_octets(wrt_volume *v) {
@@ -529,7 +543,9 @@ int wrt_volume_upload_device(wrt_volume *v, const float *dev_f32) {
 }
 
 size_t wrt_volume_bytes(const wrt_volume *v) {
-  return v ? v->vol_bytes + v->pair_bytes + v->oct_bytes + 2 * sizeof(unsigned int) : 0;
+  return v ? v->vol_bytes + v->pair_bytes + v->oct_bytes + (v->d_layers ? v->vol_bytes : 0) +
+                 2 * sizeof(unsigned int)
+           : 0;
 }
 
 int wrt_volume_destroy(wrt_volume *v) {
@@ -543,6 +559,7 @@ int wrt_volume_destroy(wrt_volume *v) {
   ctx_free(ctx, v->d_pairs, v->pair_bytes);
   ctx_free(ctx, v->d_pairs16, v->pair_bytes);
   ctx_free(ctx, v->d_oct, v->oct_bytes);
+  ctx_free(ctx, v->d_layers, v->d_layers ? v->vol_bytes : 0);
   delete v;
   return WRT_OK;
 }
@@ -711,6 +728,11 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const wrt_gri
   job.margin = sampler_margin(vol->n, o.sampler);
   job.out = dev_out;
   job.counter = ctx->d_counter;
+  if (o.sampler == WRT_SAMPLER_NEAREST && o.kernel != WRT_KERNEL_PLAIN) {
+    st = volume_ensure_layers(vol);
+    if (st) return st;
+    return plane_forward_nearest_rows(ctx, job, vol->d_layers);
+  }
   return plane_forward_plain(ctx, job);
 }
 

@@ -154,6 +154,76 @@ __global__ void __launch_bounds__(256) plane_plain_kernel(wrt::PlaneJob job, flo
   }
 }
 
+// Nearest sampler (zero_interp, radon_grid/src/interp.c:63-87), the
+// reference's default: one warp per plane walks its lattice rows in order,
+// the 32 lanes on consecutive samples of a row.  A row has one z (up to FP64
+// rounding), so its samples read one z-layer of the volume; `layers` holds the
+// volume z-major, layers[iz][iy][ix], and a warp's loads fall on adjacent
+// cells of one 64 KB layer at n = 128.  Sample positions, guard band and FP64
+// re-evaluation are the plain kernel's, expression for expression; sums: FP32
+// per lane and row, FP64 across rows, then the warp (a fixed order).
+__global__ void __launch_bounds__(256) plane_nearest_rows_kernel(wrt::PlaneJob job,
+                                                                 const float *__restrict__ layers,
+                                                                 float guard) {
+  const int lane = threadIdx.x & 31;
+  const long long nplanes = (long long)job.ndir * job.nshift;
+  const int n = job.n;
+  for (long long plane = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; plane < nplanes;
+       plane += ((long long)gridDim.x * blockDim.x) >> 5) {
+    const int is = (int)(plane / job.ndir), d = (int)(plane % job.ndir);
+    const PlaneConsts c = plane_consts(job, is, d);
+    double acc = 0.0;
+    int evaluated = 0;
+    if (c.rem >= 0.0) {
+      const double h = 0.5 * n;
+      const float du = (float)(c.a2x * h), dv = (float)(c.a2y * h), dw = (float)(c.a2z * h);
+      const float qmax = (float)n;
+      int ilo, ihi;
+      row_range(c, job.L, ilo, ihi);
+      for (int i = ilo; i <= ihi; ++i) {
+        RowGeom r;
+        if (!row_geom(c, job.L, i, r)) continue;  // uniform over the warp
+        const float ub = (float)((r.bx + 1.0) * h), vb = (float)((r.by + 1.0) * h),
+                    wb = (float)((r.bz + 1.0) * h);
+        float part = 0.0f;
+        for (int j = r.jlo + lane; j <= r.jhi; j += 32) {
+          const float jf = (float)j;
+          const float qx = fmaf(jf, du, ub), qy = fmaf(jf, dv, vb), qz = fmaf(jf, dw, wb);
+          if (wrtd::in_band(qx, guard) | wrtd::in_band(qy, guard) | wrtd::in_band(qz, guard)) {
+            const double dj = (double)j;
+            const double px = __dadd_rn(r.bx, __dmul_rn(c.a2x, dj));
+            const double py = __dadd_rn(r.by, __dmul_rn(c.a2y, dj));
+            const double pz = __dadd_rn(r.bz, __dmul_rn(c.a2z, dj));
+            acc += wrtd::exact_nearest(job.vol, n, px, py, pz);
+            ++evaluated;
+          } else if (qx > 0.0f && qy > 0.0f && qz > 0.0f && qx < qmax && qy < qmax &&
+                     qz < qmax) {
+            ++evaluated;
+            part += __ldg(layers + ((size_t)(int)qz * n + (int)qy) * n + (int)qx);
+          }
+        }
+        acc += (double)part;
+      }
+    }
+    acc = wrtd::warp_sum(acc);
+    if (lane == 0) job.out[plane] = acc * c.delta * c.delta;
+    if (job.counter) {
+      for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
+      if (lane == 0) atomicAdd(job.counter, (unsigned long long)evaluated);
+    }
+  }
+}
+
+// layers[iz][iy][ix] = v[ix][iy][iz]
+__global__ void volume_layers_kernel(const float *__restrict__ v, int n, float *__restrict__ layers) {
+  const size_t total = (size_t)n * n * n;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(k % n), iy = (int)((k / n) % n), iz = (int)(k / ((size_t)n * n));
+    layers[k] = v[((size_t)ix * n + iy) * n + iz];
+  }
+}
+
 // Exact transpose: every sample of every plane scatters g[plane] * delta^2 *
 // (its sampling weights) into an FP64 volume.  Weights follow the forward
 // kernel sample by sample (FP32 fractions outside the band, the reference's
@@ -238,6 +308,23 @@ __global__ void __launch_bounds__(256) plane_transpose_kernel(wrt::PlaneJob job,
 namespace wrt {
 
 static float guard_band(int n) { return 4.8e-7f * (float)(n > 64 ? n : 64); }
+
+int volume_layers(wrt_ctx *ctx, const float *d_vol, int n, float *d_layers) {
+  volume_layers_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(d_vol, n, d_layers);
+  ctx->launches++;
+  return check_launch(ctx, "volume_layers_kernel");
+}
+
+int plane_forward_nearest_rows(wrt_ctx *ctx, const PlaneJob &job, const float *d_layers) {
+  const long long nplanes = (long long)job.ndir * job.nshift;
+  if (nplanes == 0) return WRT_OK;
+  const float g = guard_band(job.n);  // the plain kernel's band
+  const long long want = (nplanes + 7) / 8;
+  const unsigned blocks = (unsigned)(want < ctx->sm_count * 16LL ? want : ctx->sm_count * 16LL);
+  plane_nearest_rows_kernel<<<blocks, 256, 0, ctx->stream>>>(job, d_layers, g);
+  ctx->launches++;
+  return check_launch(ctx, "plane_nearest_rows_kernel");
+}
 
 int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job) {
   const long long nplanes = (long long)job.ndir * job.nshift;

@@ -128,6 +128,9 @@ struct PlaneJob {
   const float4 *oct;    // cell octets of the volume (rotated frames), or null
 };
 int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job);
+// Nearest sampler, rows walked by whole warps over a z-major copy of the volume.
+int plane_forward_nearest_rows(wrt_ctx *ctx, const PlaneJob &job, const float *d_layers);
+int volume_layers(wrt_ctx *ctx, const float *d_vol, int n, float *d_layers);
 int plane_transpose(wrt_ctx *ctx, const PlaneJob &job, const double *d_g, double *d_vol64);
 
 // Staged plane kernel (k_staged.cu).
