@@ -579,6 +579,7 @@ def cli_compare(args):
     import subprocess
     import tempfile
 
+    load_package()
     from wrt_b200.phantom import ellipsoid_phantom
 
     sys.path.insert(0, str(ROOT))

@@ -181,10 +181,11 @@ def test_autotuner_picks_a_configuration(ctx):
 def test_nearest_row_kernel_matches_plain_kernel_and_oracle(ctx):
     """The reference's default sampler through its row kernel (lanes on
     consecutive samples, z-major layers) against the plain one-lane-per-row
-    kernel (same samples, other summation order) and the FP64 oracle."""
+    kernel (the same FP32 samples summed in other groups: FP32 rounding of the
+    partial sums, ~1e-7) and the FP64 oracle."""
     n, nphi, ntheta, nshift = 48, 24, 12, 40
     vol = ellipsoid_phantom(n, 8, 4242)
     rows = ctx.radon_grid(vol, nphi, ntheta, nshift, sampler=wrt.NEAREST)
     plain = ctx.radon_grid(vol, nphi, ntheta, nshift, sampler=wrt.NEAREST, kernel=wrt.KERNEL_PLAIN)
-    assert rel_l2(rows, plain) < 1e-12
+    assert rel_l2(rows, plain) < 1e-6
     assert rel_l2(rows, O.radon_forward(vol, nphi, ntheta, nshift, sampler=O.NEAREST)) < 1e-5
