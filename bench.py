@@ -434,21 +434,25 @@ def other_paths(wrt, ctx, phantom, steps, warmup, smem_bw, with_cpu):
     return res
 
 
-def batch_vs_one_per_launch(wrt, ctx, steps):
-    """64 FP32 volumes of uneven edge lengths {48..192}, each with its own
-    sphere grid (16-96 latitudes x twice as many longitudes, 64-256 shifts):
-    all in ONE graph-captured launch of the persistent kernel
-    (wrt_radon_forward_batch) against the same 64 requests run one
-    wrt_radon_forward_device call (staged kernel) per request.  Device time
-    with CUDA events, L2 flushed before each timed run."""
+def batch_vs_one_per_launch(wrt, ctx, steps, count=64, edges=(48, 64, 96, 128, 160, 192),
+                            lat=(16, 97), shifts=(64, 257), seed=2002):
+    """`count` FP32 volumes of uneven edge lengths (drawn from `edges`), each
+    with its own sphere grid (lat latitudes x twice as many longitudes,
+    `shifts` shifts; half-open ranges): all in ONE graph-captured launch of the
+    persistent kernel (wrt_radon_forward_batch) against the same requests run
+    one wrt_radon_forward_device call (staged kernel) per request.  Device time
+    with CUDA events, L2 flushed before each timed run.  The default is the
+    batched configuration (64 requests, n = 48..192); with small requests
+    (n = 16..48) a single request cannot fill the GPU, which is where one
+    launch for all of them pays."""
     from wrt_b200.phantom import ellipsoid_phantom
 
-    rng = np.random.default_rng(2002)
+    rng = np.random.default_rng(seed)
     reqs, keep, planes = [], [], 0
-    for k in range(64):
-        n = int(rng.choice([48, 64, 96, 128, 160, 192]))
-        nth = int(rng.integers(16, 97))
-        ns = int(rng.integers(64, 257))
+    for k in range(count):
+        n = int(rng.choice(list(edges)))
+        nth = int(rng.integers(*lat))
+        ns = int(rng.integers(*shifts))
         v = wrt.Volume(ctx, n)
         v.upload(ellipsoid_phantom(n, int(rng.integers(4, 25)), 3000 + k).astype(np.float32))
         g = wrt.Grid(ctx, 2 * nth, nth, ns)
@@ -470,10 +474,11 @@ def batch_vs_one_per_launch(wrt, ctx, steps):
     for v, g, o in keep:
         o.close(); g.close(); v.close()
     mb, mo = statistics.mean(tb), statistics.mean(to)
-    return {"requests": 64, "planes": planes, "batched_ms": mb, "one_per_launch_ms": mo,
+    return {"requests": count, "edges": sorted(set(int(r[3]) for r in reqs)),
+            "planes": planes, "batched_ms": mb, "one_per_launch_ms": mo,
             "ratio": mo / mb, "batched_plane_integrals_per_s": planes / (mb * 1e-3),
             "results_bitwise_equal": same,
-            "note": "ratio = time of 64 single-request launches / time of one batched launch"}
+            "note": f"ratio = time of {count} single-request launches / time of one batched launch"}
 
 
 # ------------------------------------------------------------ our arm
@@ -943,6 +948,9 @@ def run_ours(args, dist):
         result["paths"] = other_paths(wrt, ctx, phantom, max(3, min(args.steps, 10)), args.warmup,
                                       smem_bw, dist.rank == 0 and not args.no_cpu_baseline)
         result["batch_vs_one_per_launch"] = batch_vs_one_per_launch(wrt, ctx, 3)
+        result["batch_vs_one_per_launch_small"] = batch_vs_one_per_launch(
+            wrt, ctx, 3, count=256, edges=(16, 24, 32, 48), lat=(8, 17), shifts=(32, 65),
+            seed=2003)
     if dist.rank == 0 and dist.world == 1 and not args.no_serving_mix:
         result["serving"] = serving_mix(wrt, dev, args.mix_requests, 4000, 60 << 30)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

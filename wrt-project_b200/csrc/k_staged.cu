@@ -211,43 +211,43 @@ __device__ __forceinline__ SampleC classify(u64 q, u64 magic2, u64 half2, float 
 // One sample of the fast loop, written in PTX so that it compiles to the
 // instructions it names (the same computation in C++ came out ~8 instructions
 // longer per sample): position q = j (du, dv) + qb, the classification of
-// classify() bit for bit, the guard-band and row-end tests as predicates, the
-// shared address (bits(y' + magic) * 16 qp + 16 bits(x' + magic) + abase, or
-// the zero padding quad when the sample is not a fast one), two 16-byte loads
-// (node rows y, y+1), the z-lerp of both quad halves as pairs, the x- and
-// y-lerps, the running sum.  anyb |= 1 for a guard-band sample in the row;
-// cnt counts fast samples (measurement build).
-#define WRT_SAMPLE_STEP_PTX(COUNT_LINE)                                              \
+// classify() bit for bit, the row-end test and the guard-band test as one
+// predicate `fast`, the shared address (bits(y' + magic) * 16 qp +
+// 16 bits(x' + magic) + abase, or the zero quad), two 16-byte loads (node
+// rows y, y+1), the z-lerp of both quad halves as pairs, the x- and y-lerps,
+// the running sum.
+// A sample that is not fast (past its row's end, or in the guard band) reads
+// the zero padding quad instead.  cnt counts the lane's fast samples; a row
+// whose lanes count fewer than its length has guard-band samples.
+#define WRT_SAMPLE_STEP_PTX                                                          \
   "{\n\t"                                                                            \
   ".reg .b64 q, s, r, d, t, a01, a23, b01, b23, za, zb;\n\t"                         \
   ".reg .f32 dx, dy, m, jf, jfh, tx, ty, ca, cxa, cb, cxb, va, vb, df;\n\t"          \
   ".reg .b32 sxb, syb, addr, addr2, ax;\n\t"                                         \
-  ".reg .pred live, band, fast;\n\t"                                                 \
-  "fma.rn.f32x2 q, %3, %4, %5;\n\t"                                                  \
-  "add.rn.f32x2 s, q, %6;\n\t"                                                       \
-  "sub.rn.f32x2 r, s, %6;\n\t"                                                       \
+  ".reg .pred live, fast;\n\t"                                                       \
+  "fma.rn.f32x2 q, %2, %3, %4;\n\t"                                                  \
+  "add.rn.f32x2 s, q, %5;\n\t"                                                       \
+  "sub.rn.f32x2 r, s, %5;\n\t"                                                       \
   "sub.rn.f32x2 d, q, r;\n\t"                                                        \
-  "add.rn.f32x2 t, d, %7;\n\t"                                                       \
+  "add.rn.f32x2 t, d, %6;\n\t"                                                       \
   "mov.b64 {dx, dy}, d;\n\t"                                                         \
   "abs.f32 dx, dx;\n\t"                                                              \
   "abs.f32 dy, dy;\n\t"                                                              \
   "max.f32 m, dx, dy;\n\t"                                                           \
-  "mov.b64 {jf, jfh}, %3;\n\t"                                                       \
-  "setp.le.f32 live, jf, %9;\n\t"                                                    \
-  "setp.gt.and.f32 band, m, %8, live;\n\t"                                           \
-  "setp.le.and.f32 fast, m, %8, live;\n\t"                                           \
-  "@band or.b32 %1, %1, 1;\n\t"                                                      \
-  COUNT_LINE                                                                         \
+  "mov.b64 {jf, jfh}, %2;\n\t"                                                       \
+  "setp.le.f32 live, jf, %8;\n\t"                                                    \
+  "setp.le.and.f32 fast, m, %7, live;\n\t"                                           \
+  "@fast add.u32 %1, %1, 1;\n\t"                                                     \
   "mov.b64 {sxb, syb}, s;\n\t"                                                       \
   "shl.b32 ax, sxb, 4;\n\t"                                                          \
-  "mad.lo.u32 addr, syb, %10, %11;\n\t"                                              \
+  "mad.lo.u32 addr, syb, %9, %10;\n\t"                                               \
   "add.u32 addr, addr, ax;\n\t"                                                      \
   "selp.b32 addr, addr, %12, fast;\n\t"                                              \
-  "add.u32 addr2, addr, %10;\n\t"                                                    \
+  "add.u32 addr2, addr, %9;\n\t"                                                     \
   "ld.shared.v2.b64 {a01, a23}, [addr];\n\t"                                         \
   "ld.shared.v2.b64 {b01, b23}, [addr2];\n\t"                                        \
-  "fma.rn.f32x2 za, a23, %13, a01;\n\t"                                              \
-  "fma.rn.f32x2 zb, b23, %13, b01;\n\t"                                              \
+  "fma.rn.f32x2 za, a23, %11, a01;\n\t"                                              \
+  "fma.rn.f32x2 zb, b23, %11, b01;\n\t"                                              \
   "mov.b64 {ca, cxa}, za;\n\t"                                                       \
   "mov.b64 {cb, cxb}, zb;\n\t"                                                       \
   "mov.b64 {tx, ty}, t;\n\t"                                                         \
@@ -258,21 +258,14 @@ __device__ __forceinline__ SampleC classify(u64 q, u64 magic2, u64 half2, float 
   "add.rn.f32 %0, %0, va;\n\t"                                                       \
   "}"
 
-template <bool kCount>
 __device__ __forceinline__ void sample_step(u64 jj, u64 duv, u64 qb, u64 magic2, u64 half2,
                                             float halfband, float jbf, unsigned qp16,
-                                            unsigned abase, unsigned zaddr, u64 tz2,
-                                            float &part, unsigned &anyb, unsigned &cnt) {
-  if (kCount)
-    asm(WRT_SAMPLE_STEP_PTX("@fast add.u32 %2, %2, 1;\n\t")
-        : "+f"(part), "+r"(anyb), "+r"(cnt)
-        : "l"(jj), "l"(duv), "l"(qb), "l"(magic2), "l"(half2), "f"(halfband), "f"(jbf),
-          "r"(qp16), "r"(abase), "r"(zaddr), "l"(tz2));
-  else
-    asm(WRT_SAMPLE_STEP_PTX("")
-        : "+f"(part), "+r"(anyb), "+r"(cnt)
-        : "l"(jj), "l"(duv), "l"(qb), "l"(magic2), "l"(half2), "f"(halfband), "f"(jbf),
-          "r"(qp16), "r"(abase), "r"(zaddr), "l"(tz2));
+                                            unsigned abase, unsigned zaddr, u64 tz2, float &part,
+                                            unsigned &cnt) {
+  asm(WRT_SAMPLE_STEP_PTX
+      : "+f"(part), "+r"(cnt)
+      : "l"(jj), "l"(duv), "l"(qb), "l"(magic2), "l"(half2), "f"(halfband), "f"(jbf), "r"(qp16),
+        "r"(abase), "l"(tz2), "r"(zaddr));
 }
 #undef WRT_SAMPLE_STEP_PTX
 
@@ -579,13 +572,15 @@ __global__ void __launch_bounds__(kThreads, 1)
               // branch-free: a lane past its row's end or on a guard-band
               // sample reads the zero quads of the padding column (staged
               // column 0, node rows 0 and 1) and adds 0
-              unsigned anyb = 0, cnt = 0;
+              unsigned cnt = 0;
               u64 jj = pk2(jf0, jf0);
 #pragma unroll 4
               for (int t = 0; t < trips; ++t, jj = add2(jj, step2))
-                sample_step<kCount>(jj, duv, qb, magic2, half2, halfband, jbf, qp16, abase, smem0,
-                                    tz2, part, anyb, cnt);
-              any_band |= anyb != 0;
+                sample_step(jj, duv, qb, magic2, half2, halfband, jbf, qp16, abase, smem0, tz2,
+                            part, cnt);
+              // samples j = ja + pos + t kLanesPerRow <= jb of this lane
+              const int mine = k_jb - k_ja - pos >= 0 ? (k_jb - k_ja - pos) / kLanesPerRow + 1 : 0;
+              any_band |= (int)cnt < mine;
               if (kCount) evaluated += cnt;
             }
             // ---- guard-band samples (and whole rows in the z band) go to the

@@ -72,6 +72,36 @@ struct Corners {
   }
 };
 
+// The octet of cell c as one 32-byte load (one L1 request per sample instead
+// of two on the same sector); octet arrays come from cudaMalloc, so oct + 2c
+// is 32-byte aligned as the vector load requires.
+__device__ __forceinline__ void ld_octet(const float4 *oct, size_t c, float4 &lo, float4 &hi) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z),
+        "=f"(hi.w)
+      : "l"(oct + 2 * c));
+}
+
+// Trilinear value from a cell octet (lo: x side, hi: x+1 side, each
+// (v(y,z), v(y,z+1), v(y+1,z), v(y+1,z+1))): x, then y, then z, the order of
+// wrtd::tri32.
+__device__ __forceinline__ float octet_lerp(float4 lo, float4 hi, float tx, float ty, float tz) {
+  // (a0, b0) = lerp_x of (v(x,y,z), v(x,y,z+1)); (a1, b1) of the y+1 pair
+  const float a0 = lerp32(tx, lo.x, hi.x), b0 = lerp32(tx, lo.y, hi.y);
+  const float a1 = lerp32(tx, lo.z, hi.z), b1 = lerp32(tx, lo.w, hi.w);
+  const float e0 = lerp32(ty, a0, a1), e1 = lerp32(ty, b0, b1);
+  return lerp32(tz, e0, e1);
+}
+
+// Reference-frame value from the 8 corners c (Corners order): bilinear in
+// x, y on both layers, then the ray's z weight tz.
+__device__ __forceinline__ float layer_lerp(const float c[8], float tx, float ty, float tz) {
+  const float a0 = lerp32(tx, c[0], c[4]), a1 = lerp32(tx, c[2], c[6]);
+  const float b0 = lerp32(tx, c[1], c[5]), b1 = lerp32(tx, c[3], c[7]);
+  const float e0 = lerp32(ty, a0, a1), e1 = lerp32(ty, b0, b1);
+  return lerp32(tz, e0, e1);
+}
+
 // Trilinear at FP32 cell coordinates (outside the guard band, inside
 // [0, n-1]) from the cell octets: two 16-byte loads of one 32-byte sector,
 // then the same FP32 operations in the same order as wrtd::tri32 (x, then y,
@@ -82,12 +112,9 @@ __device__ __forceinline__ float tri32_octets(const float4 *__restrict__ oct, in
   const float tx = qx - fx, ty = qy - fy, tz = qz - fz;
   const int m = n - 1;
   const size_t c = ((size_t)(int)fx * m + (int)fy) * m + (int)fz;
-  const float4 lo = __ldg(oct + 2 * c), hi = __ldg(oct + 2 * c + 1);
-  // (a0, b0) = lerp_x of (v(x,y,z), v(x,y,z+1)); (a1, b1) of the y+1 pair
-  const float a0 = lerp32(tx, lo.x, hi.x), b0 = lerp32(tx, lo.y, hi.y);
-  const float a1 = lerp32(tx, lo.z, hi.z), b1 = lerp32(tx, lo.w, hi.w);
-  const float e0 = lerp32(ty, a0, a1), e1 = lerp32(ty, b0, b1);
-  return lerp32(tz, e0, e1);
+  float4 lo, hi;
+  ld_octet(oct, c, lo, hi);
+  return octet_lerp(lo, hi, tx, ty, tz);
 }
 
 // Ray number `ray` (0 <= ray < nslices * nshift * nphi, shift fastest) of a job.
@@ -164,47 +191,92 @@ __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, f
       dv = (float)((F[3] * ax + F[4] * ay) * h);
       dw = (float)((F[6] * ax + F[7] * ay) * h);
     }
+    // FP64 reference evaluation of sample k (interp.c:25-60 at F p(k))
+    auto exact_at = [&](int k) {
+      const double dk = (double)k;
+      double px = __dadd_rn(p0x, __dmul_rn(ax, dk));
+      double py = __dadd_rn(p0y, __dmul_rn(ay, dk));
+      double pz = __dadd_rn(p0z, __dmul_rn(__dmul_rn(delta, 0.0), dk));
+      if (FRAME) {
+        const double wx = rot_row(F, 0, px, py, pz), wy = rot_row(F, 1, px, py, pz),
+                     wz = rot_row(F, 2, px, py, pz);
+        px = wx;
+        py = wy;
+        pz = wz;
+      }
+      return wrtd::exact_trilinear(job.vol, n, px, py, pz);
+    };
+    // reference frame: bilinear in x, y on layers zc and zc+1, then the ray's
+    // z weight
+    auto layer_value = [&](float qx, float qy) {
+      const float fx = floorf(qx), fy = floorf(qy);
+      float c[8];
+      corners((int)fx, (int)fy, zc, c);
+      return layer_lerp(c, qx - fx, qy - fy, tzc);
+    };
+    // sample k: the guard-band path (FP64, the reference's arithmetic) or the
+    // FP32 trilinear value; 0 outside the cube
+    auto sample = [&](int k, float &part) {
+      const float kf = (float)k;
+      const float qx = fmaf(kf, du, ub), qy = fmaf(kf, dv, vb);
+      const float qz = FRAME ? fmaf(kf, dw, wb) : 0.5f;
+      bool band = wrtd::in_band(qx, guard) | wrtd::in_band(qy, guard);
+      if (FRAME) band |= wrtd::in_band(qz, guard);
+      if (band) {
+        acc += exact_at(k);
+      } else if (qx > 0.0f && qy > 0.0f && qx < qmax && qy < qmax &&
+                 (!FRAME || (qz > 0.0f && qz < qmax))) {
+        part += FRAME ? (job.oct ? tri32_octets(job.oct, n, qx, qy, qz)
+                                 : wrtd::tri32(job.vol, n, qx, qy, qz))
+                      : layer_value(qx, qy);
+      }
+    };
     for (int k0 = klo; k0 <= khi; k0 += 32) {
       const int k1 = min(khi, k0 + 31);
       float part = 0.0f;
-      for (int k = k0; k <= k1; ++k) {
-        const float kf = (float)k;
-        const float qx = fmaf(kf, du, ub), qy = fmaf(kf, dv, vb);
-        const float qz = FRAME ? fmaf(kf, dw, wb) : 0.5f;
-        bool band = wrtd::in_band(qx, guard) | wrtd::in_band(qy, guard);
-        if (FRAME) band |= wrtd::in_band(qz, guard);
-        if (band) {
-          const double dk = (double)k;
-          double px = __dadd_rn(p0x, __dmul_rn(ax, dk));
-          double py = __dadd_rn(p0y, __dmul_rn(ay, dk));
-          double pz = __dadd_rn(p0z, __dmul_rn(__dmul_rn(delta, 0.0), dk));
-          if (FRAME) {
-            double wx = rot_row(F, 0, px, py, pz), wy = rot_row(F, 1, px, py, pz),
-                   wz = rot_row(F, 2, px, py, pz);
-            px = wx;
-            py = wy;
-            pz = wz;
+      int k = k0;
+      // rotated frame: four samples at a time with all their octet loads
+      // issued together (the same values, added in the same order, as one at
+      // a time); a group with a guard-band sample takes the one-at-a-time
+      // path.  (The reference frame's corner loads are coalesced already, and
+      // batching them only costs it occupancy.)
+      if (FRAME && job.oct) {
+        for (; k + 3 <= k1; k += 4) {
+          float qx[4], qy[4], qz[4];
+          bool band = false, in[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float kf = (float)(k + u);
+            qx[u] = fmaf(kf, du, ub);
+            qy[u] = fmaf(kf, dv, vb);
+            qz[u] = fmaf(kf, dw, wb);
+            band |= wrtd::in_band(qx[u], guard) | wrtd::in_band(qy[u], guard) |
+                    wrtd::in_band(qz[u], guard);
+            in[u] = qx[u] > 0.0f && qy[u] > 0.0f && qz[u] > 0.0f && qx[u] < qmax &&
+                    qy[u] < qmax && qz[u] < qmax;
           }
-          acc += wrtd::exact_trilinear(job.vol, n, px, py, pz);
-        } else if (qx > 0.0f && qy > 0.0f && qx < qmax && qy < qmax &&
-                   (!FRAME || (qz > 0.0f && qz < qmax))) {
-          if (FRAME) {
-            part += job.oct ? tri32_octets(job.oct, n, qx, qy, qz) : wrtd::tri32(job.vol, n, qx, qy, qz);
-          } else {
-            // bilinear in x, y on layers zc and zc+1, then the ray's z weight
-            const float fx = floorf(qx), fy = floorf(qy);
-            const float tx = qx - fx, ty = qy - fy;
-            float c[8];
-            corners((int)fx, (int)fy, zc, c);
-            const float c000 = c[0], c001 = c[1], c010 = c[2], c011 = c[3], c100 = c[4],
-                        c101 = c[5], c110 = c[6], c111 = c[7];
-            const float a0 = wrtd::lerp32(tx, c000, c100), a1 = wrtd::lerp32(tx, c010, c110);
-            const float b0 = wrtd::lerp32(tx, c001, c101), b1 = wrtd::lerp32(tx, c011, c111);
-            const float e0 = wrtd::lerp32(ty, a0, a1), e1 = wrtd::lerp32(ty, b0, b1);
-            part += wrtd::lerp32(tzc, e0, e1);
+          if (band) {
+#pragma unroll 1
+            for (int u = 0; u < 4; ++u) sample(k + u, part);
+            continue;
           }
+          float4 lo[4], hi[4];
+          float tx[4], ty[4], tz[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float fx = floorf(qx[u]), fy = floorf(qy[u]), fz = floorf(qz[u]);
+            tx[u] = qx[u] - fx, ty[u] = qy[u] - fy, tz[u] = qz[u] - fz;
+            lo[u] = hi[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (in[u])
+              ld_octet(job.oct, ((size_t)(int)fx * (n - 1) + (int)fy) * (n - 1) + (int)fz, lo[u],
+                       hi[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (in[u]) part += octet_lerp(lo[u], hi[u], tx[u], ty[u], tz[u]);
         }
       }
+      for (; k <= k1; ++k) sample(k, part);
       acc += (double)part;
     }
   }

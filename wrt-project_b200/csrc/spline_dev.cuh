@@ -252,7 +252,7 @@ __device__ __forceinline__ adj_u64 adj_sub2(adj_u64 a, adj_u64 b) {
 
 // Warp w (0 <= w < adjoint_warps(n)) over directions [dbeg, dbeg + nd) of an
 // n^3 backprojection; lines[d] holds direction d's ns-1 records.
-template <int V>
+template <int V, int U = 1>
 __device__ __forceinline__ void adjoint_block(const float4 *__restrict__ lines, int ns, int dbeg,
                                               int nd, const AdjDirs &dirs, int n, long long w,
                                               int lane, double *__restrict__ out) {
@@ -282,7 +282,7 @@ __device__ __forceinline__ void adjoint_block(const float4 *__restrict__ lines, 
     float acc[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) acc[v] = 0.0f;
-#pragma unroll 1
+#pragma unroll U
     for (int j = j0; j < j1; ++j) {
       const float4 *line = lines + (size_t)(dbeg + j) * line_len;
       const int4 hd = dirs.hd[j];
