@@ -149,9 +149,40 @@ def test_staged_agrees_with_plain(ctx):
     assert rel_l2(a, b) < 2e-6
 
 
-def test_staged_rejects_nearest(ctx, vol24):
-    with pytest.raises(wrt.WrtError):
-        ctx.radon_grid(vol24, 4, 4, 4, sampler=O.NEAREST, kernel=wrt.KERNEL_STAGED)
+# The reference's default sampler (zero_interp) through the staged kernel: one
+# FP32 value per cell of a z-layer in shared memory, the reference's lattice
+# [-2n, 2n)^2 unless stated.
+NEAREST_CASES = [
+    (24, (16, 8, 12), 0),
+    (33, (9, 7, 13), 0),      # odd n: z = 0 is a cell boundary (guard-band rows)
+    (64, (16, 8, 20), 64),
+    (224, (4, 3, 5), 0),      # two y-tiles
+]
+
+
+@pytest.mark.parametrize("n,grid,L", NEAREST_CASES)
+def test_staged_nearest_matches_oracle_and_plain(ctx, n, grid, L):
+    vol = ellipsoid_phantom(n, 8, 2100 + n)
+    got = ctx.radon_grid(vol, *grid, sampler=O.NEAREST, half_extent=L, kernel=wrt.KERNEL_STAGED)
+    ref = O.radon_forward(vol, *grid, sampler=O.NEAREST, half_extent=L)
+    assert rel_l2(got, ref) < TOL_L2
+    assert rel_max(got, ref) < 1e-4
+    # the plain kernel takes the same FP32 samples (or the same FP64 ones in the
+    # guard band) and sums them in other groups: FP32 rounding of the partial sums
+    plain = ctx.radon_grid(vol, *grid, sampler=O.NEAREST, half_extent=L, kernel=wrt.KERNEL_PLAIN)
+    assert rel_l2(got, plain) < 1e-6
+
+
+def test_staged_nearest_random_volume_nonzero_faces(ctx, volrand):
+    got = ctx.radon_grid(volrand, 8, 6, 9, sampler=O.NEAREST, kernel=wrt.KERNEL_STAGED)
+    ref = O.radon_forward(volrand, 8, 6, 9, sampler=O.NEAREST)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+def test_staged_nearest_is_the_default_and_deterministic(ctx, vol24):
+    a = ctx.radon_grid(vol24, 16, 8, 12, sampler=O.NEAREST)
+    b = ctx.radon_grid(vol24, 16, 8, 12, sampler=O.NEAREST, kernel=wrt.KERNEL_STAGED)
+    assert np.array_equal(a, b)
 
 
 def test_every_staged_tile_configuration_matches_oracle(ctx):
@@ -178,14 +209,3 @@ def test_autotuner_picks_a_configuration(ctx):
     out.close(); grid.close(); vol.close()
 
 
-def test_nearest_row_kernel_matches_plain_kernel_and_oracle(ctx):
-    """The reference's default sampler through its row kernel (lanes on
-    consecutive samples, z-major layers) against the plain one-lane-per-row
-    kernel (the same FP32 samples summed in other groups: FP32 rounding of the
-    partial sums, ~1e-7) and the FP64 oracle."""
-    n, nphi, ntheta, nshift = 48, 24, 12, 40
-    vol = ellipsoid_phantom(n, 8, 4242)
-    rows = ctx.radon_grid(vol, nphi, ntheta, nshift, sampler=wrt.NEAREST)
-    plain = ctx.radon_grid(vol, nphi, ntheta, nshift, sampler=wrt.NEAREST, kernel=wrt.KERNEL_PLAIN)
-    assert rel_l2(rows, plain) < 1e-6
-    assert rel_l2(rows, O.radon_forward(vol, nphi, ntheta, nshift, sampler=O.NEAREST)) < 1e-5

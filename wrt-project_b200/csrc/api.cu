@@ -643,38 +643,42 @@ int wrt_grid_destroy(wrt_grid *g) {
 
 namespace {
 
-// Staged-kernel launch of one request; see k_staged.cu.
+// Staged-kernel launch of one request; see k_staged.cu.  Trilinear: the
+// volume's layer pairs; nearest: its z-major cell layers (FP32 storage).
 int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, int L,
-                         double *dev_out) {
-  int st = volume_ensure_pairs(vol);
+                         double *dev_out, bool nearest) {
+  int st = nearest ? volume_ensure_layers(vol) : volume_ensure_pairs(vol);
   if (st) return st;
   const int n = vol->n;
   int th = 0, qp = 0;
-  const int smem = staged_smem_bytes(n, &th, &qp);
+  const int smem =
+      nearest ? staged_smem_bytes_nearest(n, &th, &qp) : staged_smem_bytes(n, &th, &qp);
   StagedReq r = {};
   const bool bf16 = vol->storage == WRT_STORAGE_BF16;
-  r.pairs = bf16 ? (const void *)vol->d_pairs16 : (const void *)vol->d_pairs;
+  r.pairs = nearest ? (const void *)vol->d_layers
+                    : bf16 ? (const void *)vol->d_pairs16 : (const void *)vol->d_pairs;
   r.vol = bf16 ? (const void *)vol->d_vol16 : (const void *)vol->d_vol;
   r.storage = vol->storage;
+  r.nearest = nearest ? 1 : 0;
   r.dir = grid->d_dir;
   r.dir32 = grid->d_dir32;
   r.shift = grid->d_shift;
   r.shift32 = grid->d_shift32;
   r.acc = reinterpret_cast<unsigned long long *>(dev_out);
   r.n = n;
-  r.pitch2 = vol->pitch;
+  r.pitch2 = nearest ? n : vol->pitch;
   r.qpitch = qp;
   r.tile_h = th;
   r.ndir = grid->nphi * grid->ntheta;
   r.nshift = grid->nshift;
   r.L = L;
-  r.crop_r2 = trilinear_crop_r2(vol->r2, n);
-  r.guard = staged_guard(n, L, r.crop_r2);
+  r.crop_r2 = nearest ? nearest_crop_r2(vol->r2, n) : trilinear_crop_r2(vol->r2, n);
+  r.guard = staged_guard(n, L, r.crop_r2, nearest);
   r.scale = fixed_point_scale(vol->maxabs, L);
   StagedItem *d_items = nullptr;
   const int *d_nitems = nullptr;
   int nitems = 0;
-  st = staged_items_cached(ctx, n, th, r.crop_r2, r.ndir, &d_items, &d_nitems, &nitems);
+  st = staged_items_cached(ctx, n, th, r.crop_r2, r.ndir, &d_items, &d_nitems, &nitems, nearest);
   if (st) return st;
   st = staged_scratch(ctx, sizeof(StagedReq));
   if (st) return st;
@@ -684,8 +688,9 @@ int radon_forward_staged(wrt_ctx *ctx, wrt_volume *vol, const wrt_grid *grid, in
   cudaError_t e = cudaMemsetAsync(dev_out, 0, sizeof(double) * nout, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged output reset");
   if (nitems > 0) {
-    st = plane_staged_launch(ctx, ctx->stream, (const StagedReq *)ctx->staged_req, d_items,
-                             d_nitems, smem, ctx->staged_next);
+    st = (nearest ? plane_staged_launch_nearest : plane_staged_launch)(
+        ctx, ctx->stream, (const StagedReq *)ctx->staged_req, d_items, d_nitems, smem,
+        ctx->staged_next);
     if (st) return st;
   }
   const double delta = 1.0 / n;
@@ -707,14 +712,18 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const wrt_gri
   if (opts) o = *opts;
   const int L = o.half_extent ? o.half_extent : 2 * vol->n;
   int th = 0, qp = 0;
-  const bool staged_ok = o.sampler == WRT_SAMPLER_TRILINEAR && vol->n >= 4 &&
-                         staged_smem_bytes(vol->n, &th, &qp) > 0;
-  if (o.kernel == WRT_KERNEL_STAGED && !staged_ok)
-    return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "staged kernel needs the trilinear sampler");
-  if (vol->storage == WRT_STORAGE_BF16 && (o.kernel == WRT_KERNEL_PLAIN || !staged_ok))
+  const bool nearest = o.sampler == WRT_SAMPLER_NEAREST;
+  const bool staged_ok =
+      vol->n >= 4 && (nearest ? vol->storage == WRT_STORAGE_F32 &&
+                                    staged_smem_bytes_nearest(vol->n, &th, &qp) > 0
+                              : staged_smem_bytes(vol->n, &th, &qp) > 0);
+  if (vol->storage == WRT_STORAGE_BF16 && (o.kernel == WRT_KERNEL_PLAIN || nearest || !staged_ok))
     return fail(ctx, WRT_ERR_INVALID_ARGUMENT,
                 "BF16 volumes are sampled by the staged kernel (trilinear sampler) only");
-  if (o.kernel != WRT_KERNEL_PLAIN && staged_ok) return radon_forward_staged(ctx, vol, grid, L, dev_out);
+  if (o.kernel == WRT_KERNEL_STAGED && !staged_ok)
+    return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "staged kernel: volume edge below 4");
+  if (o.kernel != WRT_KERNEL_PLAIN && staged_ok)
+    return radon_forward_staged(ctx, vol, grid, L, dev_out, nearest);
   PlaneJob job = {};
   job.vol = vol->d_vol;
   job.n = vol->n;
@@ -728,11 +737,6 @@ int wrt_radon_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const wrt_gri
   job.margin = sampler_margin(vol->n, o.sampler);
   job.out = dev_out;
   job.counter = ctx->d_counter;
-  if (o.sampler == WRT_SAMPLER_NEAREST && o.kernel != WRT_KERNEL_PLAIN) {
-    st = volume_ensure_layers(vol);
-    if (st) return st;
-    return plane_forward_nearest_rows(ctx, job, vol->d_layers);
-  }
   return plane_forward_plain(ctx, job);
 }
 

@@ -154,154 +154,9 @@ __global__ void __launch_bounds__(256) plane_plain_kernel(wrt::PlaneJob job, flo
   }
 }
 
-// Nearest sampler (zero_interp, radon_grid/src/interp.c:63-87), the
-// reference's default: one warp per plane walks its lattice rows in order,
-// the 32 lanes on consecutive samples of a row.  A row has one z (up to FP64
-// rounding), so its samples read one z-layer of the volume; `layers` holds the
-// volume z-major, layers[iz][iy][ix], and a warp's loads fall on adjacent
-// cells of one 64 KB layer at n = 128.
-//
-// Row set-up (the FP64 geometry of row_geom) runs one row per lane, 32 rows at
-// a time; the warp then walks those rows one after another with the row's
-// constants broadcast by shuffle.  A sample's cell is round(q - 1/2), q the
-// FP32 cell coordinate of the plain kernel, by the 1.5 * 2^23 rounding
-// constant (no float-to-integer conversions): with e = (q - 1/2) -
-// round(q - 1/2), q lies within the guard band g of a cell boundary exactly
-// when |e| > 1/2 - g, and such samples take the reference's FP64 arithmetic
-// as in the plain kernel.  Outside the band round(q - 1/2) = floor(q) is the
-// reference's cell, and the sample is inside the cube exactly when that cell
-// is in [0, n).  Sums: FP32 per lane and row, FP64 across rows, then the warp
-// (a fixed order).
-__global__ void __launch_bounds__(256) plane_nearest_rows_kernel(wrt::PlaneJob job,
-                                                                 const float *__restrict__ layers,
-                                                                 float guard) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __shared__ double s_base[8][32][3];  // FP64 row base points of the warp's 32 rows
-  const long long nplanes = (long long)job.ndir * job.nshift;
-  const int n = job.n;
-  constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
-  constexpr int kMagicBits = 0x4B400000;
-  const float halfband = 0.5f - guard;
-  const unsigned mb = (unsigned)kMagicBits, un = (unsigned)n;
-  // cell (x, y, z) from the rounded bits: ((bz n + by) n + bx) + koff, mod 2^32
-  const unsigned koff =
-      0u - (unsigned)kMagicBits * ((unsigned)n * (unsigned)n + (unsigned)n + 1u);
-  for (long long plane = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; plane < nplanes;
-       plane += ((long long)gridDim.x * blockDim.x) >> 5) {
-    const int is = (int)(plane / job.ndir), d = (int)(plane % job.ndir);
-    const PlaneConsts c = plane_consts(job, is, d);
-    double acc = 0.0;
-    int evaluated = 0;
-    if (c.rem >= 0.0) {
-      const double h = 0.5 * n;
-      const float du = (float)(c.a2x * h), dv = (float)(c.a2y * h), dw = (float)(c.a2z * h);
-      int ilo, ihi;
-      row_range(c, job.L, ilo, ihi);
-      for (int i0 = ilo; i0 <= ihi; i0 += 32) {
-        RowGeom r;
-        const bool ok = i0 + lane <= ihi && row_geom(c, job.L, i0 + lane, r);
-        // q - 1/2 at j = 0 (the plain kernel's row origin, shifted exactly
-        // for origins >= 1/4, within 2^-26 below)
-        float ub = 0.0f, vb = 0.0f, wb = 0.0f;
-        int jlo = 1, jhi = 0;
-        if (ok) {
-          ub = (float)((r.bx + 1.0) * h) - 0.5f;
-          vb = (float)((r.by + 1.0) * h) - 0.5f;
-          wb = (float)((r.bz + 1.0) * h) - 0.5f;
-          jlo = r.jlo;
-          jhi = r.jhi;
-          s_base[warp][lane][0] = r.bx;
-          s_base[warp][lane][1] = r.by;
-          s_base[warp][lane][2] = r.bz;
-        }
-        __syncwarp();
-        for (unsigned live = __ballot_sync(0xffffffffu, ok); live; live &= live - 1) {
-          const int src = __ffs(live) - 1;
-          const float rub = __shfl_sync(0xffffffffu, ub, src);
-          const float rvb = __shfl_sync(0xffffffffu, vb, src);
-          const float rwb = __shfl_sync(0xffffffffu, wb, src);
-          const int rjlo = __shfl_sync(0xffffffffu, jlo, src),
-                    rjhi = __shfl_sync(0xffffffffu, jhi, src);
-          float part = 0.0f;
-          // sample j of the row: the reference's FP64 path in the guard
-          // band, else the FP32 cell (0 outside the cube)
-          auto sample = [&](int j) {
-            const float jf = (float)j;
-            const float qx = fmaf(jf, du, rub), qy = fmaf(jf, dv, rvb), qz = fmaf(jf, dw, rwb);
-            const float sx = qx + kMagic, sy = qy + kMagic, sz = qz + kMagic;
-            const float ex = qx - (sx - kMagic), ey = qy - (sy - kMagic), ez = qz - (sz - kMagic);
-            if (fmaxf(fmaxf(fabsf(ex), fabsf(ey)), fabsf(ez)) > halfband) {
-              const double dj = (double)j;
-              const double px = __dadd_rn(s_base[warp][src][0], __dmul_rn(c.a2x, dj));
-              const double py = __dadd_rn(s_base[warp][src][1], __dmul_rn(c.a2y, dj));
-              const double pz = __dadd_rn(s_base[warp][src][2], __dmul_rn(c.a2z, dj));
-              acc += wrtd::exact_nearest(job.vol, n, px, py, pz);
-              ++evaluated;
-            } else {
-              const unsigned bx = (unsigned)__float_as_int(sx);
-              const unsigned by = (unsigned)__float_as_int(sy);
-              const unsigned bz = (unsigned)__float_as_int(sz);
-              if ((bx - mb < un) & (by - mb < un) & (bz - mb < un)) {
-                ++evaluated;
-                part += __ldg(layers + ((bz * un + by) * un + bx + koff));
-              }
-            }
-          };
-          // four samples per lane (j, j+32, j+64, j+96) at a time, their
-          // loads issued together and their values added in the same order
-          // as one at a time; a group with a guard-band sample goes one at a
-          // time
-          int j = rjlo + lane;
-          for (; j <= rjhi; j += 128) {
-            float jf = (float)j;
-            unsigned idx[4];
-            bool in[4], band = false;
-#pragma unroll
-            for (int u = 0; u < 4; ++u, jf += 32.0f) {
-              const float qx = fmaf(jf, du, rub), qy = fmaf(jf, dv, rvb), qz = fmaf(jf, dw, rwb);
-              const float sx = qx + kMagic, sy = qy + kMagic, sz = qz + kMagic;
-              const float ex = qx - (sx - kMagic), ey = qy - (sy - kMagic),
-                          ez = qz - (sz - kMagic);
-              const bool live = j + 32 * u <= rjhi;
-              band |= live & (fmaxf(fmaxf(fabsf(ex), fabsf(ey)), fabsf(ez)) > halfband);
-              const unsigned bx = (unsigned)__float_as_int(sx);
-              const unsigned by = (unsigned)__float_as_int(sy);
-              const unsigned bz = (unsigned)__float_as_int(sz);
-              in[u] = live & (bx - mb < un) & (by - mb < un) & (bz - mb < un);
-              idx[u] = (bz * un + by) * un + bx + koff;
-            }
-            if (band) {
-#pragma unroll 1
-              for (int u = 0; u < 4; ++u)
-                if (j + 32 * u <= rjhi) sample(j + 32 * u);
-              continue;
-            }
-            float v[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = in[u] ? __ldg(layers + idx[u]) : 0.0f;
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-              if (in[u]) {
-                ++evaluated;
-                part += v[u];
-              }
-          }
-          acc += (double)part;
-        }
-        __syncwarp();
-      }
-    }
-    acc = wrtd::warp_sum(acc);
-    if (lane == 0) job.out[plane] = acc * c.delta * c.delta;
-    if (job.counter) {
-      for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
-      if (lane == 0) atomicAdd(job.counter, (unsigned long long)evaluated);
-    }
-  }
-}
-
-// layers[iz][iy][ix] = v[ix][iy][iz]
-__global__ void volume_layers_kernel(const float *__restrict__ v, int n, float *__restrict__ layers) {
+// layers[iz][iy][ix] = v[ix][iy][iz] (the staged nearest sampler's cell layers)
+__global__ void volume_layers_kernel(const float *__restrict__ v, int n,
+                                     float *__restrict__ layers) {
   const size_t total = (size_t)n * n * n;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
        k += (size_t)gridDim.x * blockDim.x) {
@@ -399,17 +254,6 @@ int volume_layers(wrt_ctx *ctx, const float *d_vol, int n, float *d_layers) {
   volume_layers_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(d_vol, n, d_layers);
   ctx->launches++;
   return check_launch(ctx, "volume_layers_kernel");
-}
-
-int plane_forward_nearest_rows(wrt_ctx *ctx, const PlaneJob &job, const float *d_layers) {
-  const long long nplanes = (long long)job.ndir * job.nshift;
-  if (nplanes == 0) return WRT_OK;
-  const float g = guard_band(job.n);  // the plain kernel's band
-  const long long want = (nplanes + 7) / 8;
-  const unsigned blocks = (unsigned)(want < ctx->sm_count * 16LL ? want : ctx->sm_count * 16LL);
-  plane_nearest_rows_kernel<<<blocks, 256, 0, ctx->stream>>>(job, d_layers, g);
-  ctx->launches++;
-  return check_launch(ctx, "plane_nearest_rows_kernel");
 }
 
 int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job) {

@@ -23,6 +23,15 @@
 //   Persistent CTAs (one per SM) pull items from a global counter; the host
 //   orders items by estimated cost, largest first.
 //
+// Nearest sampler (zero_interp, radon_grid/src/interp.c:63-87, the
+// reference's default): the same items, rows, classification and sums over
+// the n^3 cells instead of the n - 1 node intervals (h = n/2 cells per unit
+// length); a row's samples lie in one cell layer, whose y-tile is staged as
+// one FP32 value per cell from the volume's z-major copy (all 128 rows of a
+// layer fit at n = 128), and a sample is one 4-byte load of cell
+// round(q - 1/2) = floor(q).  Guard-band samples take the reference's FP64
+// zero_interp arithmetic.
+//
 // Arithmetic: coordinates and interpolation use the packed FP32 pair
 // instructions of sm_100 (fma/add/sub .f32x2) on (x, y) and on the quad
 // halves.
@@ -185,6 +194,7 @@ __device__ __noinline__ double exact_sample(const wrt::StagedReq &R, int d, int 
                               __dmul_rn(__dmul_rn(delta, D[7]), dj));
   const double pz = __dadd_rn(__dadd_rn(__dmul_rn(s, D[2]), __dmul_rn(__dmul_rn(delta, D[5]), di)),
                               __dmul_rn(__dmul_rn(delta, D[8]), dj));
+  if (R.nearest) return wrtd::exact_nearest(static_cast<const float *>(R.vol), R.n, px, py, pz);
   return R.storage == WRT_STORAGE_BF16
              ? wrtd::exact_trilinear(static_cast<const __nv_bfloat16 *>(R.vol), R.n, px, py, pz)
              : wrtd::exact_trilinear(static_cast<const float *>(R.vol), R.n, px, py, pz);
@@ -269,6 +279,46 @@ __device__ __forceinline__ void sample_step(u64 jj, u64 duv, u64 qb, u64 magic2,
 }
 #undef WRT_SAMPLE_STEP_PTX
 
+// The nearest sampler's sample (zero_interp): the same position and
+// classification, the cell round(q) (that is floor of the cell coordinate),
+// one 4-byte load of the staged cell value (or of the zero cell), the sum.
+#define WRT_NEAREST_STEP_PTX                                                         \
+  "{\n\t"                                                                            \
+  ".reg .b64 q, s, r, d;\n\t"                                                        \
+  ".reg .f32 dx, dy, m, jf, jfh, v;\n\t"                                             \
+  ".reg .b32 sxb, syb, addr, ax;\n\t"                                                \
+  ".reg .pred live, fast;\n\t"                                                       \
+  "fma.rn.f32x2 q, %2, %3, %4;\n\t"                                                  \
+  "add.rn.f32x2 s, q, %5;\n\t"                                                       \
+  "sub.rn.f32x2 r, s, %5;\n\t"                                                       \
+  "sub.rn.f32x2 d, q, r;\n\t"                                                        \
+  "mov.b64 {dx, dy}, d;\n\t"                                                         \
+  "abs.f32 dx, dx;\n\t"                                                              \
+  "abs.f32 dy, dy;\n\t"                                                              \
+  "max.f32 m, dx, dy;\n\t"                                                           \
+  "mov.b64 {jf, jfh}, %2;\n\t"                                                       \
+  "setp.le.f32 live, jf, %7;\n\t"                                                    \
+  "setp.le.and.f32 fast, m, %6, live;\n\t"                                           \
+  "@fast add.u32 %1, %1, 1;\n\t"                                                     \
+  "mov.b64 {sxb, syb}, s;\n\t"                                                       \
+  "shl.b32 ax, sxb, 2;\n\t"                                                          \
+  "mad.lo.u32 addr, syb, %8, %9;\n\t"                                                \
+  "add.u32 addr, addr, ax;\n\t"                                                      \
+  "selp.b32 addr, addr, %10, fast;\n\t"                                              \
+  "ld.shared.f32 v, [addr];\n\t"                                                     \
+  "add.rn.f32 %0, %0, v;\n\t"                                                        \
+  "}"
+
+__device__ __forceinline__ void nearest_step(u64 jj, u64 duv, u64 qb, u64 magic2, float halfband,
+                                             float jbf, unsigned qp4, unsigned abase,
+                                             unsigned zaddr, float &part, unsigned &cnt) {
+  asm(WRT_NEAREST_STEP_PTX
+      : "+f"(part), "+r"(cnt)
+      : "l"(jj), "l"(duv), "l"(qb), "l"(magic2), "f"(halfband), "f"(jbf), "r"(qp4), "r"(abase),
+        "r"(zaddr));
+}
+#undef WRT_NEAREST_STEP_PTX
+
 // FP64 reference evaluation of `count` queued guard-band samples of direction
 // d, one per lane, each added to its plane as a fixed-point integer.  Returns
 // the number of samples this lane evaluated.
@@ -285,8 +335,11 @@ __device__ __forceinline__ int exact_queue_flush(const wrt::StagedReq &R, int d,
 // kThreads: CTA size (one CTA per SM); kGroup: lattice rows a warp walks at
 // once (32/kGroup lanes per row, on consecutive samples); kShiftsPerLane:
 // shifts a lane enumerates per pass (a pass covers 32*kShiftsPerLane shifts);
-// kCount: count the samples evaluated (measurement build).
-template <int kThreads, int kGroup, int kShiftsPerLane, bool kCount>
+// kCount: count the samples evaluated (measurement build); kNear: the nearest
+// sampler (n cells per axis, one staged FP32 value per cell of a z-layer,
+// rows grouped by the cell layer of their z) instead of trilinear (n - 1
+// cells between nodes, layer pairs staged as quads).
+template <int kThreads, int kGroup, int kShiftsPerLane, bool kCount, bool kNear = false>
 __global__ void __launch_bounds__(kThreads, 1)
     plane_staged_kernel(const wrt::StagedReq *__restrict__ reqs,
                         const wrt::StagedItem *__restrict__ items,
@@ -326,7 +379,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (it >= nitems) break;
     const wrt::StagedItem item = items[it];
     const wrt::StagedReq &R = reqs[item.req];
-    const int n = R.n, W = n - 1;
+    const int n = R.n, W = kNear ? n : n - 1;  // cells per axis
     const int qp = R.qpitch;
     const int y0 = item.tile * R.tile_h;
     const int H = min(R.tile_h, W - y0);
@@ -341,7 +394,18 @@ __global__ void __launch_bounds__(kThreads, 1)
       s_item_geo[3] = item.layer == W - 1 ? (double)W + kZBand : (double)(item.layer + 1);
     }
     // ---- stage layer pair (iz, iz+1), node rows y0 .. y0+H, cells -2 .. W+1
-    {
+    // (nearest: cell layer iz, cell rows y0 .. y0+H-1, one float per cell)
+    if (kNear) {
+      const float *src = static_cast<const float *>(R.pairs) +
+                         ((size_t)item.layer * n * R.pitch2 + (size_t)y0 * R.pitch2);
+      float *cells = reinterpret_cast<float *>(quads);
+      const int wide = W + 2 * kPadX;
+      const int total = H * wide;
+      for (int k = tid; k < total; k += kThreads) {
+        const int yy = k / wide, xc = k - yy * wide, x = xc - kPadX;
+        cells[yy * qp + xc] = (x >= 0 && x < W) ? __ldg(src + (size_t)yy * R.pitch2 + x) : 0.0f;
+      }
+    } else {
       const size_t base = (size_t)item.layer * n * R.pitch2 + (size_t)y0 * R.pitch2;
       const float2 *src = static_cast<const float2 *>(R.pairs) + base;
       const __nv_bfloat162 *src16 = static_cast<const __nv_bfloat162 *>(R.pairs) + base;
@@ -370,11 +434,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     // Cell coordinates are held relative to the grid's centre cell C (halves
     // their magnitude and so their FP32 rounding, which sets the guard band).
     const int C = W / 2;
-    // shared address of cell (x, row y) = sbase + 16 * (yrel * qp + bits(x' + magic)),
-    // yrel = bits(y' + magic) - yoff; as one expression (mod 2^32):
-    //   bits(y' + magic) * 16 qp + 16 bits(x' + magic) + abase
-    const unsigned sbase = smem0 + 16u * (unsigned)(kPadX + C - kMagicBits);
-    const unsigned qp16 = 16u * (unsigned)qp;
+    // shared address of cell (x, row y) = sbase + E * (yrel * qp + bits(x' + magic)),
+    // yrel = bits(y' + magic) - yoff, E the element size (16, nearest 4); as
+    // one expression (mod 2^32):
+    //   bits(y' + magic) * E qp + E bits(x' + magic) + abase
+    constexpr unsigned kElem = kNear ? 4u : 16u;
+    const unsigned sbase = smem0 + kElem * (unsigned)(kPadX + C - kMagicBits);
+    const unsigned qp16 = kElem * (unsigned)qp;
     const int yoff = kMagicBits - C + y0;
     const unsigned abase = sbase - qp16 * (unsigned)yoff;
     for (;;) {
@@ -476,7 +542,7 @@ __global__ void __launch_bounds__(kThreads, 1)
               const int jm = (int)floorf(sqrtf(rem) * nf) + 1;
               jlo = max(-L, -jm);
               jhi = min(L - 1, jm);
-              if (!clip_lin(ub, du, inv_du, -1.5f - C, (float)(n - C) - 0.5f, jlo, jhi) ||
+              if (!clip_lin(ub, du, inv_du, -1.5f - C, (float)(W + 1 - C) - 0.5f, jlo, jhi) ||
                   !clip_lin(vb, dv, inv_dv, (float)(y0 - C) - 1.5f, (float)(y0 + H - C) + 0.5f,
                             jlo, jhi)) {
                 jlo = 1;
@@ -574,10 +640,16 @@ __global__ void __launch_bounds__(kThreads, 1)
               // column 0, node rows 0 and 1) and adds 0
               unsigned cnt = 0;
               u64 jj = pk2(jf0, jf0);
+              if (kNear) {
 #pragma unroll 4
-              for (int t = 0; t < trips; ++t, jj = add2(jj, step2))
-                sample_step(jj, duv, qb, magic2, half2, halfband, jbf, qp16, abase, smem0, tz2,
-                            part, cnt);
+                for (int t = 0; t < trips; ++t, jj = add2(jj, step2))
+                  nearest_step(jj, duv, qb, magic2, halfband, jbf, qp16, abase, smem0, part, cnt);
+              } else {
+#pragma unroll 4
+                for (int t = 0; t < trips; ++t, jj = add2(jj, step2))
+                  sample_step(jj, duv, qb, magic2, half2, halfband, jbf, qp16, abase, smem0, tz2,
+                              part, cnt);
+              }
               // samples j = ja + pos + t kLanesPerRow <= jb of this lane
               const int mine = k_jb - k_ja - pos >= 0 ? (k_jb - k_ja - pos) / kLanesPerRow + 1 : 0;
               any_band |= (int)cnt < mine;
@@ -672,12 +744,25 @@ int staged_smem_bytes(int n, int *tile_h, int *qpitch) {
   return (th + 1) * qp * 16;
 }
 
+int staged_smem_bytes_nearest(int n, int *tile_h, int *qpitch) {
+  int qp = n + 2 * kPadX;
+  if (!(qp & 1)) ++qp;  // odd pitch: a row of cells and the next start in different banks
+  const int rows_max = kStagedSmemMax / (qp * 4);  // cell rows that fit
+  if (rows_max < 2) return -1;
+  const int ntiles = (n + rows_max - 1) / rows_max;
+  const int th = (n + ntiles - 1) / ntiles;  // balanced tiles of <= rows_max cell rows
+  *tile_h = th;
+  *qpitch = qp;
+  return th * qp * 4;
+}
+
 namespace {
-template <int T, int G, int K>
+template <int T, int G, int K, bool NEAR = false>
 int launch_cfg(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
                const StagedItem *d_items, const int *d_nitems, int max_smem, int *d_next) {
   const bool count = ctx->d_counter != nullptr;
-  auto kern = count ? plane_staged_kernel<T, G, K, true> : plane_staged_kernel<T, G, K, false>;
+  auto kern = count ? plane_staged_kernel<T, G, K, true, NEAR>
+                    : plane_staged_kernel<T, G, K, false, NEAR>;
   max_smem += (T / 32) * wrt::kStagedWarpSmemQuads * 16;  // per-warp row tables and queues
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "staged kernel smem attribute");
@@ -715,6 +800,12 @@ int plane_staged_launch(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_re
   }
 }
 
+int plane_staged_launch_nearest(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
+                                const StagedItem *d_items, const int *d_nitems, int max_smem,
+                                int *d_next) {
+  return launch_cfg<1024, 8, 2, true>(ctx, stream, d_reqs, d_items, d_nitems, max_smem, d_next);
+}
+
 int plane_finalize(wrt_ctx *ctx, double *out, long long count, double factor) {
   const int blocks = ctx->sm_count * 4;
   plane_finalize_kernel<<<blocks, 256, 0, ctx->stream>>>(out, count, factor);
@@ -725,10 +816,11 @@ int plane_finalize(wrt_ctx *ctx, double *out, long long count, double factor) {
 // Work items of one request, largest estimated cost first.  Cost of a
 // (layer, tile): voxels of the tile's slab inside the crop radius.
 void staged_items_costed(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
-                         double weight, std::vector<std::pair<double, StagedItem>> &out) {
-  const int W = n - 1;
+                         double weight, std::vector<std::pair<double, StagedItem>> &out,
+                         bool nearest) {
+  const int W = nearest ? n : n - 1;  // cells per axis
   const int ntiles = (W + tile_h - 1) / tile_h;
-  const double h = 2.0 / (n - 1);
+  const double h = 2.0 / W;
   for (int iz = 0; iz < W; ++iz) {
     const double z = -1.0 + h * (iz + 0.5);
     for (int t = 0; t < ntiles; ++t) {
@@ -753,9 +845,9 @@ void staged_items_costed(int req, int n, int tile_h, float crop_r2, int ndir, in
 }
 
 void staged_items(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
-                  std::vector<StagedItem> &out) {
+                  std::vector<StagedItem> &out, bool nearest) {
   std::vector<std::pair<double, StagedItem>> v;
-  staged_items_costed(req, n, tile_h, crop_r2, ndir, dir_chunk, 1.0, v);
+  staged_items_costed(req, n, tile_h, crop_r2, ndir, dir_chunk, 1.0, v, nearest);
   std::stable_sort(v.begin(), v.end(),
                    [](const std::pair<double, StagedItem> &a,
                       const std::pair<double, StagedItem> &b) { return a.first > b.first; });
@@ -769,19 +861,19 @@ struct ItemList {
   size_t bytes = 0;
 };
 struct StagedCache {
-  std::map<std::tuple<int, int, unsigned, int>, ItemList> lists;
+  std::map<std::tuple<int, int, unsigned, int, bool>, ItemList> lists;
 };
 }  // namespace
 
 // Device copy of the item list of one geometry: a 16-byte header holding the
 // item count (the kernel reads it from there), then the items.
 int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir,
-                        StagedItem **d_items, const int **d_nitems, int *nitems) {
+                        StagedItem **d_items, const int **d_nitems, int *nitems, bool nearest) {
   if (!ctx->staged_cache) ctx->staged_cache = new StagedCache();
   StagedCache *c = static_cast<StagedCache *>(ctx->staged_cache);
   unsigned bits;
   memcpy(&bits, &crop_r2, sizeof(bits));
-  const auto key = std::make_tuple(n, tile_h, bits, ndir);
+  const auto key = std::make_tuple(n, tile_h, bits, ndir, nearest);
   auto it = c->lists.find(key);
   if (it == c->lists.end()) {
     if (c->lists.size() > 64) {  // bounded: drop everything, rebuild on demand
@@ -790,7 +882,7 @@ int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir
       c->lists.clear();
     }
     std::vector<StagedItem> items;
-    staged_items(0, n, tile_h, crop_r2, ndir, kStagedDirChunk, items);
+    staged_items(0, n, tile_h, crop_r2, ndir, kStagedDirChunk, items, nearest);
     ItemList l;
     l.count = (int)items.size();
     l.bytes = 16 + sizeof(StagedItem) * items.size();

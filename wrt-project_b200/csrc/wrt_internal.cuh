@@ -128,8 +128,8 @@ struct PlaneJob {
   const float4 *oct;    // cell octets of the volume (rotated frames), or null
 };
 int plane_forward_plain(wrt_ctx *ctx, const PlaneJob &job);
-// Nearest sampler, rows walked by whole warps over a z-major copy of the volume.
-int plane_forward_nearest_rows(wrt_ctx *ctx, const PlaneJob &job, const float *d_layers);
+// z-major copy layers[iz][iy][ix] of an FP32 volume (the nearest sampler's
+// staged cell layers).
 int volume_layers(wrt_ctx *ctx, const float *d_vol, int n, float *d_layers);
 int plane_transpose(wrt_ctx *ctx, const PlaneJob &job, const double *d_g, double *d_vol64);
 
@@ -144,6 +144,8 @@ struct StagedReq {
   unsigned long long *acc; // [nshift][ndir] fixed-point accumulators (the output buffer)
   int n, pitch2, qpitch, tile_h, ndir, nshift, L;
   int storage;             // wrt_storage of pairs / vol
+  int nearest;             // 1: zero_interp on the n^3 cells; pairs = z-major cell layers
+                           // [iz][y][pitch2] (FP32), cells of tile_h rows staged per item
   float guard, crop_r2;
   double scale;            // fixed-point scale 2^k
 };
@@ -156,6 +158,9 @@ struct StagedConfig {
 extern const StagedConfig kStagedConfigs[];
 extern const int kNumStagedConfigs;
 int staged_smem_bytes(int n, int *tile_h, int *qpitch);
+// The nearest sampler's tile: tile_h cell rows of (n + 4) FP32 cells, pitch
+// qpitch floats; bytes of the tile or -1.
+int staged_smem_bytes_nearest(int n, int *tile_h, int *qpitch);
 // Guard band (in cells) of the staged kernel's x / y cell fractions.  Cell
 // coordinates are held relative to the centre cell C = (n-1)/2 (rounded
 // down); q' = fma(j, du, q0') with q0' and du rounded once from FP64, so
@@ -166,8 +171,8 @@ int staged_smem_bytes(int n, int *tile_h, int *qpitch);
 // a cell boundary (where the reference's cell index and fraction can
 // disagree) or on a cube face lies inside it.  Host and device compute it
 // alike (the batched path sets it on the device from the volume statistics).
-__host__ __device__ inline float staged_guard(int n, int L, float crop_r2) {
-  const double h = 0.5 * (n - 1);
+__host__ __device__ inline float staged_guard(int n, int L, float crop_r2, bool nearest = false) {
+  const double h = 0.5 * (nearest ? n : n - 1);  // cells per unit length
   const double ulp = 1.0 / 8388608.0;  // 2^-23 relative
   const double bound = 0.5 * ulp * (sqrt((double)crop_r2) * h + 1.0) +
                        0.5 * ulp * (h + 3.0) + 0.5 * ulp * 0.5 * L;
@@ -182,15 +187,21 @@ constexpr int kStagedWarpSmemQuads = 96;
 int plane_staged_launch(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
                         const StagedItem *d_items, const int *d_nitems, int max_smem,
                         int *d_next);
+// The nearest sampler's staged launch (one request; default tile shape).
+int plane_staged_launch_nearest(wrt_ctx *ctx, cudaStream_t stream, const StagedReq *d_reqs,
+                                const StagedItem *d_items, const int *d_nitems, int max_smem,
+                                int *d_next);
 int plane_finalize(wrt_ctx *ctx, double *out, long long count, double factor);
 // Work items of one request (layer x y-tile x direction chunk) with their
 // estimated cost (staged voxels inside the crop radius x directions x weight).
 void staged_items_costed(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
-                         double weight, std::vector<std::pair<double, StagedItem>> &out);
+                         double weight, std::vector<std::pair<double, StagedItem>> &out,
+                         bool nearest = false);
 void staged_items(int req, int n, int tile_h, float crop_r2, int ndir, int dir_chunk,
-                  std::vector<StagedItem> &out);
+                  std::vector<StagedItem> &out, bool nearest = false);
 int staged_items_cached(wrt_ctx *ctx, int n, int tile_h, float crop_r2, int ndir,
-                        StagedItem **d_items, const int **d_nitems, int *nitems);
+                        StagedItem **d_items, const int **d_nitems, int *nitems,
+                        bool nearest = false);
 int staged_scratch(wrt_ctx *ctx, size_t req_bytes);
 void staged_release(wrt_ctx *ctx);
 
@@ -374,6 +385,14 @@ __host__ __device__ inline double fixed_point_scale(float maxabs, int L) {
 __host__ __device__ inline float trilinear_crop_r2(float r2, int n) {
   const double h = 2.0 / (n - 1);
   const double rc = sqrt((double)r2) + (sqrt(3.0) * h + 1e-6);
+  return (float)fmin(rc * rc * (1.0 + 1e-6), 3.0 + 1e-5);
+}
+
+// The same for the nearest sampler: a lattice point farther than sqrt(r2)
+// plus the margin of the plain kernel's nearest crop (two cell diagonals of
+// the cell grid and one of the node grid) lies in a zero cell.
+__host__ __device__ inline float nearest_crop_r2(float r2, int n) {
+  const double rc = sqrt((double)r2) + (sqrt(3.0) * (4.0 / n + 2.0 / (n - 1)) + 1e-6);
   return (float)fmin(rc * rc * (1.0 + 1e-6), 3.0 + 1e-5);
 }
 
