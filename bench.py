@@ -982,6 +982,10 @@ PATHS = {
                   "plane integrals/s",
                   "radon_reduction, rays 128 layers x 128 shifts x 128 angles -> 64x128 sphere "
                   "grid x 256 shifts (ray shift grid decoupled: spline over 128 offsets)"),
+    "nearest": ("plane integrals/s @128^3 (64x128 sphere grid x 256 shifts, nearest sampler, "
+                "512^2 lattice)", "plane integrals/s",
+                "radon_grid with the reference's defaults: zero_interp, lattice [-2n, 2n)^2 with "
+                "step 1/n, 128^3 volume of 16 seeded ellipsoids, 64x128 sphere grid x 256 shifts"),
     "adjoint": ("voxels/s of the backprojection to 128^3 (64x128 sphere grid x 256 shifts)",
                 "voxels/s",
                 "radon3d_adjoint, seeded N(0,1) Radon data 64x128 sphere grid x 256 shifts -> "
@@ -1019,6 +1023,9 @@ def run_path(args, dist):
         rays = ctx.ray_grid(vol, n, 128, 128)
         call = lambda: ctx.radon_reduction(rays, NSHIFT, NTHETA)
         units, h2d, d2h = NSHIFT * NPHI * NTHETA, rays.nbytes, NSHIFT * NPHI * NTHETA * 8
+    elif args.path == "nearest":
+        call = lambda: ctx.radon_grid(vol, NPHI, NTHETA, NSHIFT, sampler=wrt.NEAREST)
+        units, h2d, d2h = NSHIFT * NPHI * NTHETA, vol.nbytes, NSHIFT * NPHI * NTHETA * 8
     else:
         radon = rng.standard_normal((NSHIFT, NPHI, NTHETA))
         call = lambda: ctx.radon3d_adjoint(radon, n)
@@ -1056,6 +1063,13 @@ def run_path(args, dist):
             m = units
             got = O.ray_forward(vol, n, 128, 128, frame=frame, nthreads=cores).reshape(-1)
             ours = result.reshape(-1)
+        elif args.path == "nearest":
+            m = 1024
+            idx = rng.integers(0, units, size=m)
+            phi, theta, _, shift = O.radon_grid(NPHI, NTHETA, NSHIFT)
+            got = ref.plane_integrals(vol, phi[(idx // NTHETA) % NPHI], theta[idx % NTHETA],
+                                      shift[idx // (NPHI * NTHETA)], cores)
+            ours = result.reshape(-1)[idx]
         elif args.path == "reduction":
             m = 4096
             idx = rng.integers(0, units, size=m)

@@ -960,10 +960,11 @@ int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const double *f
   st = ws_get(ctx, WS_TABLE, sizeof(double) * tab.size(), &dtab);
   // a copy from pageable memory returns once the data is staged
   if (!st) st = h2d(ctx, dtab, tab.data(), sizeof(double) * tab.size(), "ray grid");
-  // z-slices read one layer pair each: the volume's layer pairs (built once);
-  // rotated layers read cell octets (built once)
+  // samples read the cell octets (one 32-byte sector each; built once per
+  // volume); in the reference frame the guard-band-free groups do, and single
+  // samples read the layer pairs (built once) as before
   if (!st && identity) st = volume_ensure_pairs(vol);
-  if (!st && !identity) st = volume_ensure_octets(vol);
+  if (!st) st = volume_ensure_octets(vol);
   if (st) return st;
   RayJob job = {};
   job.vol = vol->d_vol;
@@ -983,9 +984,8 @@ int wrt_ray_forward_device(wrt_ctx *ctx, const wrt_volume *cvol, const double *f
   if (identity) {
     job.pairs = vol->d_pairs;
     job.pitch = vol->pitch;
-  } else {
-    job.oct = vol->d_oct;
   }
+  job.oct = vol->d_oct;
   return ray_forward(ctx, job);
 }
 

@@ -47,31 +47,6 @@ __device__ __forceinline__ double rot_row(const double *F, int r, double x, doub
                    __dmul_rn(F[3 * r + 2], z));
 }
 
-// The 8 corners (x, y, z) .. (x+1, y+1, z+1) of a reference-frame sample:
-// from the layer pairs P[z][y][x] = (v(x,y,z), v(x,y,z+1)) when the volume has
-// them -- a slice reads one z-layer pair, whose rows are contiguous in x, so
-// neighbouring samples share cache lines -- else from the volume v[x][y][z],
-// where a slice uses 2 of the 32 z values of every line it touches.
-struct Corners {
-  const float *vol;
-  const float2 *pairs;
-  int n, pitch;
-  __device__ __forceinline__ void operator()(int ix, int iy, int zc, float c[8]) const {
-    if (pairs) {
-      const float2 *p = pairs + ((size_t)zc * n + iy) * pitch + ix;
-      const float2 a = __ldg(p), b = __ldg(p + pitch), d = __ldg(p + 1), e = __ldg(p + pitch + 1);
-      c[0] = a.x, c[1] = a.y, c[2] = b.x, c[3] = b.y, c[4] = d.x, c[5] = d.y, c[6] = e.x,
-      c[7] = e.y;
-    } else {
-      const float *p = vol + ((size_t)ix * n + iy) * n + zc;
-      const size_t sx = (size_t)n * n;
-      c[0] = __ldg(p), c[1] = __ldg(p + 1), c[2] = __ldg(p + n), c[3] = __ldg(p + n + 1);
-      c[4] = __ldg(p + sx), c[5] = __ldg(p + sx + 1), c[6] = __ldg(p + sx + n);
-      c[7] = __ldg(p + sx + n + 1);
-    }
-  }
-};
-
 // The octet of cell c as one 32-byte load (one L1 request per sample instead
 // of two on the same sector); octet arrays come from cudaMalloc, so oct + 2c
 // is 32-byte aligned as the vector load requires.
@@ -93,29 +68,19 @@ __device__ __forceinline__ float octet_lerp(float4 lo, float4 hi, float tx, floa
   return lerp32(tz, e0, e1);
 }
 
-// Reference-frame value from the 8 corners c (Corners order): bilinear in
-// x, y on both layers, then the ray's z weight tz.
-__device__ __forceinline__ float layer_lerp(const float c[8], float tx, float ty, float tz) {
-  const float a0 = lerp32(tx, c[0], c[4]), a1 = lerp32(tx, c[2], c[6]);
-  const float b0 = lerp32(tx, c[1], c[5]), b1 = lerp32(tx, c[3], c[7]);
-  const float e0 = lerp32(ty, a0, a1), e1 = lerp32(ty, b0, b1);
-  return lerp32(tz, e0, e1);
-}
+constexpr float kRayMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr unsigned kRayMagicBits = 0x4B400000u;
 
-// Trilinear at FP32 cell coordinates (outside the guard band, inside
-// [0, n-1]) from the cell octets: two 16-byte loads of one 32-byte sector,
-// then the same FP32 operations in the same order as wrtd::tri32 (x, then y,
-// then z; the x and y steps on packed pairs), so the value is bitwise tri32's.
-__device__ __forceinline__ float tri32_octets(const float4 *__restrict__ oct, int n, float qx,
-                                              float qy, float qz) {
-  const float fx = floorf(qx), fy = floorf(qy), fz = floorf(qz);
-  const float tx = qx - fx, ty = qy - fy, tz = qz - fz;
-  const int m = n - 1;
-  const size_t c = ((size_t)(int)fx * m + (int)fy) * m + (int)fz;
-  float4 lo, hi;
-  ld_octet(oct, c, lo, hi);
-  return octet_lerp(lo, hi, tx, ty, tz);
-}
+// A sample's cell: bits of round(q') + 1.5 * 2^23 per axis (q' = the FP32
+// cell coordinate minus 1/2, so round(q') = floor of the coordinate outside
+// the guard band), the fractions t = q' - round(q') + 1/2, whether the
+// coordinate lies within the guard band of a cell boundary, and whether the
+// cell is inside the node grid.
+struct RayCell {
+  unsigned bx, by, bz;
+  float tx, ty, tz;
+  bool band, in;
+};
 
 // Ray number `ray` (0 <= ray < nslices * nshift * nphi, shift fastest) of a job.
 template <bool FRAME>
@@ -124,7 +89,6 @@ __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, f
   const int ip = (int)((ray / job.nshift) % job.nphi);
   const int iz = (int)(ray / ((long long)job.nphi * job.nshift));
   const int n = job.n;
-  const Corners corners{job.vol, job.pairs, n, job.pitch};
   const double *T = job.trig + 4 * ip;
   const double s = job.shift[is];
   const double dz = 2.0 / (job.nslices - 1);                     // ray_grid.c:244
@@ -150,7 +114,6 @@ __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, f
     any = klo <= khi;
   }
   const double h = 0.5 * (n - 1);
-  const float qmax = (float)(n - 1);
   const double *F = job.frame;  // kernel parameter space
   if (any && !FRAME) {
     any = clip_axis(p0x, ax, klo, khi) && clip_axis(p0y, ay, klo, khi) && fabs(zslice) <= 1.0;
@@ -206,54 +169,90 @@ __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, f
       }
       return wrtd::exact_trilinear(job.vol, n, px, py, pz);
     };
-    // reference frame: bilinear in x, y on layers zc and zc+1, then the ray's
-    // z weight
-    auto layer_value = [&](float qx, float qy) {
-      const float fx = floorf(qx), fy = floorf(qy);
-      float c[8];
-      corners((int)fx, (int)fy, zc, c);
-      return layer_lerp(c, qx - fx, qy - fy, tzc);
+    // Every path locates a sample the same way and interpolates its 8
+    // corners in one order (octet_lerp: x, then y, then z), whether the
+    // corners come from the cell octets, the layer pairs or the volume, so a
+    // ray's value does not depend on which of them the job carries.
+    // q' = q - 1/2 at k = 0 (one more rounding of at most half an ulp, well
+    // inside the guard band's allowance for the FP32 coordinates)
+    ub -= 0.5f;
+    vb -= 0.5f;
+    wb -= 0.5f;
+    const float halfband = 0.5f - guard;
+    const unsigned mb = kRayMagicBits, um = (unsigned)(n - 1);
+    auto locate = [&](int k) {
+      RayCell c;
+      const float kf = (float)k;
+      const float qx = fmaf(kf, du, ub), qy = fmaf(kf, dv, vb);
+      const float sx = qx + kRayMagic, sy = qy + kRayMagic;
+      const float ex = qx - (sx - kRayMagic), ey = qy - (sy - kRayMagic);
+      c.bx = __float_as_uint(sx);
+      c.by = __float_as_uint(sy);
+      c.tx = ex + 0.5f;
+      c.ty = ey + 0.5f;
+      float m = fmaxf(fabsf(ex), fabsf(ey));
+      c.in = (c.bx - mb < um) & (c.by - mb < um);
+      if (FRAME) {
+        const float qz = fmaf(kf, dw, wb), sz = qz + kRayMagic;
+        const float ez = qz - (sz - kRayMagic);
+        c.bz = __float_as_uint(sz);
+        c.tz = ez + 0.5f;
+        m = fmaxf(m, fabsf(ez));
+        c.in &= c.bz - mb < um;
+      } else {
+        c.bz = mb + (unsigned)zc;  // the ray's z cell, reference arithmetic
+        c.tz = tzc;
+      }
+      c.band = m > halfband;
+      return c;
+    };
+    // the 8 corners of an inside cell in octet order
+    auto gather = [&](const RayCell &c, float4 &lo, float4 &hi) {
+      const unsigned ix = c.bx - mb, iy = c.by - mb, izc = c.bz - mb;
+      if (job.oct) {
+        ld_octet(job.oct, ((size_t)ix * (n - 1) + iy) * (n - 1) + izc, lo, hi);
+      } else if (!FRAME && job.pairs) {
+        // one z-layer pair: rows contiguous in x
+        const float2 *p = job.pairs + ((size_t)izc * n + iy) * job.pitch + ix;
+        const float2 a = __ldg(p), b = __ldg(p + job.pitch), d = __ldg(p + 1),
+                     e = __ldg(p + job.pitch + 1);
+        lo = make_float4(a.x, a.y, b.x, b.y);
+        hi = make_float4(d.x, d.y, e.x, e.y);
+      } else {
+        const float *p = job.vol + ((size_t)ix * n + iy) * n + izc;
+        const size_t sx = (size_t)n * n;
+        lo = make_float4(__ldg(p), __ldg(p + 1), __ldg(p + n), __ldg(p + n + 1));
+        hi = make_float4(__ldg(p + sx), __ldg(p + sx + 1), __ldg(p + sx + n),
+                         __ldg(p + sx + n + 1));
+      }
     };
     // sample k: the guard-band path (FP64, the reference's arithmetic) or the
     // FP32 trilinear value; 0 outside the cube
     auto sample = [&](int k, float &part) {
-      const float kf = (float)k;
-      const float qx = fmaf(kf, du, ub), qy = fmaf(kf, dv, vb);
-      const float qz = FRAME ? fmaf(kf, dw, wb) : 0.5f;
-      bool band = wrtd::in_band(qx, guard) | wrtd::in_band(qy, guard);
-      if (FRAME) band |= wrtd::in_band(qz, guard);
-      if (band) {
+      const RayCell c = locate(k);
+      if (c.band) {
         acc += exact_at(k);
-      } else if (qx > 0.0f && qy > 0.0f && qx < qmax && qy < qmax &&
-                 (!FRAME || (qz > 0.0f && qz < qmax))) {
-        part += FRAME ? (job.oct ? tri32_octets(job.oct, n, qx, qy, qz)
-                                 : wrtd::tri32(job.vol, n, qx, qy, qz))
-                      : layer_value(qx, qy);
+      } else if (c.in) {
+        float4 lo, hi;
+        gather(c, lo, hi);
+        part += octet_lerp(lo, hi, c.tx, c.ty, c.tz);
       }
     };
     for (int k0 = klo; k0 <= khi; k0 += 32) {
       const int k1 = min(khi, k0 + 31);
       float part = 0.0f;
       int k = k0;
-      // rotated frame: four samples at a time with all their octet loads
+      // with the cell octets: four samples at a time with all their loads
       // issued together (the same values, added in the same order, as one at
-      // a time); a group with a guard-band sample takes the one-at-a-time
-      // path.  (The reference frame's corner loads are coalesced already, and
-      // batching them only costs it occupancy.)
-      if (FRAME && job.oct) {
+      // a time); a group with a guard-band sample takes the one-at-a-time path
+      if (job.oct) {
         for (; k + 3 <= k1; k += 4) {
-          float qx[4], qy[4], qz[4];
-          bool band = false, in[4];
+          RayCell c[4];
+          bool band = false;
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const float kf = (float)(k + u);
-            qx[u] = fmaf(kf, du, ub);
-            qy[u] = fmaf(kf, dv, vb);
-            qz[u] = fmaf(kf, dw, wb);
-            band |= wrtd::in_band(qx[u], guard) | wrtd::in_band(qy[u], guard) |
-                    wrtd::in_band(qz[u], guard);
-            in[u] = qx[u] > 0.0f && qy[u] > 0.0f && qz[u] > 0.0f && qx[u] < qmax &&
-                    qy[u] < qmax && qz[u] < qmax;
+            c[u] = locate(k + u);
+            band |= c[u].band;
           }
           if (band) {
 #pragma unroll 1
@@ -261,19 +260,14 @@ __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, f
             continue;
           }
           float4 lo[4], hi[4];
-          float tx[4], ty[4], tz[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            const float fx = floorf(qx[u]), fy = floorf(qy[u]), fz = floorf(qz[u]);
-            tx[u] = qx[u] - fx, ty[u] = qy[u] - fy, tz[u] = qz[u] - fz;
             lo[u] = hi[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (in[u])
-              ld_octet(job.oct, ((size_t)(int)fx * (n - 1) + (int)fy) * (n - 1) + (int)fz, lo[u],
-                       hi[u]);
+            if (c[u].in) gather(c[u], lo[u], hi[u]);
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u)
-            if (in[u]) part += octet_lerp(lo[u], hi[u], tx[u], ty[u], tz[u]);
+            if (c[u].in) part += octet_lerp(lo[u], hi[u], c[u].tx, c[u].ty, c[u].tz);
         }
       }
       for (; k <= k1; ++k) sample(k, part);
