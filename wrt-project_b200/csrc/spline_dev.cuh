@@ -74,15 +74,12 @@ __device__ __forceinline__ void spline_line_centred(const double *__restrict__ y
   }
 }
 
-__device__ __forceinline__ float spline_eval(const float4 *__restrict__ line, int ns, float q,
-                                             float h2_6) {
-  // q = (s + 1)/h in knot units
-  float fi = floorf(q);
-  fi = fminf(fmaxf(fi, 0.0f), (float)(ns - 2));
-  const float b = q - fi, a = 1.0f - b;
-  const float4 c = __ldg(line + (int)fi);
+// Value of reduction record c at fraction b of its knot interval.
+__device__ __forceinline__ float spline_value(const float4 c, float b, float h2_6) {
+  const float a = 1.0f - b;
   return fmaf(a, c.x, b * c.y) + ((a * a - 1.0f) * a * c.z + (b * b - 1.0f) * b * c.w) * h2_6;
 }
+
 
 __device__ __forceinline__ float cubic_centred(const float4 c, float u) {
   return fmaf(u, fmaf(u, fmaf(u, c.w, c.z), c.y), c.x);
@@ -91,9 +88,12 @@ __device__ __forceinline__ float cubic_centred(const float4 c, float u) {
 // ------------------------------------------------------------ reduction
 // radon_reduction (radon_reduction/slicing.c:80-119) of Radon sample k
 // (is, iphi, itheta), order of reduction.c:215-229, from the reduction lines
-// [iz][iphi][ns_ray-1] of the ray data: geometry in FP64 with the reference's
-// expressions, spline values and the quadratic in z (slicing.c:62-74) in
-// FP32.  Returns the integral; *evaluated counts the slice samples taken.
+// [iz][iphi][ns_ray-1] of the ray data, by one thread: geometry in FP64 with
+// the reference's expressions, spline values and the quadratic in z
+// (slicing.c:62-74) in FP32, summed in FP64 in tau order.  No conversion
+// instructions in the sample loop: the layer index and the knot interval are
+// rounded by the 1.5 * 2^52 and 1.5 * 2^23 constants.  Returns the integral;
+// *evaluated counts the slice samples taken.
 __device__ __forceinline__ double reduction_one(const float4 *__restrict__ lines, int ngrid,
                                                 int ns_ray, int nphi,
                                                 const double *__restrict__ shift,
@@ -108,6 +108,9 @@ __device__ __forceinline__ double reduction_one(const float4 *__restrict__ lines
   const float hs = 2.0f / (float)(ns_ray - 1);
   const float inv_hs = 1.0f / hs;
   const float h2_6 = hs * hs / 6.0f;
+  const float last = (float)(ns_ray - 2);
+  constexpr double kMagic52 = 6755399441055744.0;  // 1.5 * 2^52
+  constexpr float kMagic23 = 12582912.0f;          // 1.5 * 2^23
   const int half = 2 * ngrid;
   // |tau| <= sqrt(1 - p^2) bounds the samples that pass slicing.c:110
   int kmax = half;
@@ -119,6 +122,7 @@ __device__ __forceinline__ double reduction_one(const float4 *__restrict__ lines
   double acc = 0.0;
   int evaluated = 0;
   const size_t line_len = (size_t)(ns_ray - 1);
+  const size_t layer = (size_t)nphi * line_len;
   for (int itau = -kmax; itau <= kmax; ++itau) {
     const double tau = __dmul_rn((double)itau, dtau);
     const double z = __dadd_rn(__dmul_rn(p, ct), __dmul_rn(tau, st));
@@ -126,21 +130,30 @@ __device__ __forceinline__ double reduction_one(const float4 *__restrict__ lines
     if ((fabs(__dadd_rn(__dmul_rn(tau, tau), __dmul_rn(p, p))) > 1.0) || (fabs(z) > 1.0) ||
         (fabs(s) > 1.0))
       continue;
-    // layer index of slicing.c:15-20, (int)((z + 1) / delta_z): by the
-    // reciprocal, and by the division itself where the quotient lies within
-    // 1e-9 of an integer (the reciprocal's error is ~1e-14 there)
+    // layer index of slicing.c:15-20, (int)((z + 1) / delta_z): the
+    // reciprocal's quotient qz >= 0 rounded by the 1.5 * 2^52 constant and
+    // corrected down when below its rounding, and the division itself where
+    // qz lies within 1e-9 of an integer (the reciprocal's error is ~1e-14)
     const double z1 = __dadd_rn(z, 1.0), qz = z1 * inv_dz;
-    int iz = (int)qz;
-    if (fabs(qz - rint(qz)) < 1e-9) iz = (int)__ddiv_rn(z1, delta_z);
+    const double tq = qz + kMagic52;
+    const double dq = qz - (tq - kMagic52);  // qz - round(qz), exact
+    int iz = __double2loint(tq) - (dq < 0.0 ? 1 : 0);
+    if (fabs(dq) < 1e-9) iz = (int)__ddiv_rn(z1, delta_z);
     if (iz == ngrid - 1) iz -= 1;
     const double z0 = __dadd_rn(-1.0, __dmul_rn(delta_z, (double)iz));
     const float f = (float)((z - z0) * inv_dz);
+    // knot interval floor(q) clamped to the line and the fraction b, q = (s + 1)/h
+    // in knot units (round(q - 1/2) = floor(q) but at the knots, where both
+    // neighbouring intervals give the knot's value)
     const float q = (float)(s + 1.0) * inv_hs;
-    const float4 *l0 = lines + ((size_t)iz * nphi + ip) * line_len;
-    const float v0 = spline_eval(l0, ns_ray, q, h2_6);
-    const float v1 = spline_eval(l0 + (size_t)nphi * line_len, ns_ray, q, h2_6);
-    const float v2 =
-        iz >= ngrid - 2 ? 0.0f : spline_eval(l0 + 2 * (size_t)nphi * line_len, ns_ray, q, h2_6);
+    const float fi = fminf(fmaxf(((q - 0.5f) + kMagic23) - kMagic23, 0.0f), last);
+    const float b = q - fi;
+    const float4 *rec = lines + ((size_t)iz * nphi + ip) * line_len +
+                        (__float_as_int(fi + kMagic23) - 0x4B400000);
+    const float4 c0 = __ldg(rec), c1 = __ldg(rec + layer);
+    const float4 c2 = iz >= ngrid - 2 ? make_float4(0.f, 0.f, 0.f, 0.f) : __ldg(rec + 2 * layer);
+    const float v0 = spline_value(c0, b, h2_6), v1 = spline_value(c1, b, h2_6);
+    const float v2 = iz >= ngrid - 2 ? 0.0f : spline_value(c2, b, h2_6);
     // quadratic through (z0, v0), (z0+dz, v1), (z0+2dz, v2) at z0 + f dz
     const float val = v0 + f * (v1 - v0) + 0.5f * f * (f - 1.0f) * (v2 - 2.0f * v1 + v0);
     acc += (double)val;
