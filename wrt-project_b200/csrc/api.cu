@@ -280,6 +280,8 @@ int wrt_ctx_destroy(wrt_ctx *ctx) {
   if (ctx->dropin_grid) wrt_grid_destroy(ctx->dropin_grid);
   laplace_release(ctx);
   for (int r = 0; r < WS_ROLES; ++r) ctx_free(ctx, ctx->ws[r], ctx->ws_bytes[r]);
+  pinned_release(ctx);
+  host_pool_destroy(ctx->host_pool);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WRT_OK;
@@ -392,7 +394,7 @@ int wrt_copy_to_device(wrt_ctx *ctx, void *dst, const void *src, size_t bytes) {
 
 int wrt_copy_to_host(wrt_ctx *ctx, void *dst, const void *src, size_t bytes) {
   if (!ctx || !dst || !src) return WRT_ERR_INVALID_ARGUMENT;
-  return d2h_sync(ctx, dst, src, bytes, "copy to host");
+  return d2h_staged_sync(ctx, dst, src, bytes, "copy to host");
 }
 
 int wrt_measure_smem_bandwidth(wrt_ctx *ctx, double *bytes_per_s) {
@@ -517,16 +519,18 @@ int wrt_volume_upload(wrt_volume *v, const double *f64, const float *f32) {
   const bool bf16 = v->storage == WRT_STORAGE_BF16;
   // staging (and the FP32 copy a BF16 volume is rounded from) in the context's
   // workspace; the upload waits for the statistics, so the buffers are free
-  // again when it returns
-  const size_t in_bytes = count * (f64 ? sizeof(double) : sizeof(float));
+  // again when it returns.  FP64 values are rounded to FP32 on the host while
+  // they are staged (to nearest, as the device conversion would), so the
+  // device receives FP32 either way.
+  const size_t in_bytes = count * sizeof(float);
   void *stage = nullptr, *vol32 = nullptr;
   st = ws_get(ctx, WS_STAGE, in_bytes, &stage);
   if (!st && bf16) st = ws_get(ctx, WS_IN, count * sizeof(float), &vol32);
   float *dst = bf16 ? static_cast<float *>(vol32) : v->d_vol;
-  if (!st) st = h2d(ctx, stage, f64 ? (const void *)f64 : (const void *)f32, in_bytes, "volume upload");
   if (!st)
-    st = f64 ? volume_from_f64(ctx, static_cast<double *>(stage), v->n, dst, v->d_stats)
-             : volume_from_f32(ctx, static_cast<float *>(stage), v->n, dst, v->d_stats);
+    st = f64 ? h2d_staged_rounded(ctx, static_cast<float *>(stage), f64, count, "volume upload")
+             : h2d_staged(ctx, stage, f32, in_bytes, "volume upload");
+  if (!st) st = volume_from_f32(ctx, static_cast<float *>(stage), v->n, dst, v->d_stats);
   if (!st && bf16) st = volume_to_bf16(ctx, dst, v->n, v->d_vol16, v->d_stats);
   if (!st) st = volume_finish_upload(v);
   return st;
@@ -902,7 +906,7 @@ int wrt_radon_grid(wrt_ctx *ctx, const double *volume, int n, int nphi, int nthe
   if (!st) st = dropin_grid(ctx, nphi, ntheta, nshift, &grid);
   if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
   if (!st) st = wrt_radon_forward_device(ctx, vol, grid, opts, static_cast<double *>(dout));
-  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "radon_grid result");
+  if (!st) st = d2h_staged_sync(ctx, out, dout, sizeof(double) * nout, "radon_grid result");
   return st;
 }
 
@@ -937,7 +941,7 @@ int wrt_radon_transpose(wrt_ctx *ctx, const double *g, int n, int nphi, int nthe
     job.margin = 0.0;
     st = plane_transpose(ctx, job, dg.as<double>(), dvol.as<double>());
   }
-  if (!st) st = d2h_sync(ctx, out_volume, dvol.p, sizeof(double) * nvox, "transpose result");
+  if (!st) st = d2h_staged_sync(ctx, out_volume, dvol.p, sizeof(double) * nvox, "transpose result");
   if (grid) wrt_grid_destroy(grid);
   return st;
 }
@@ -1003,7 +1007,7 @@ int wrt_ray_grid(wrt_ctx *ctx, const double *volume, int n, int nslices, int nsh
   if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
   if (!st) st = wrt_ray_forward_device(ctx, vol, frame, nslices, nshift, nphi,
                                        static_cast<double *>(dout));
-  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "ray_grid result");
+  if (!st) st = d2h_staged_sync(ctx, out, dout, sizeof(double) * nout, "ray_grid result");
   return st;
 }
 
@@ -1031,11 +1035,11 @@ int wrt_radon_reduction(wrt_ctx *ctx, const double *rays, int ngrid, int nshift_
   st = dropin_grid(ctx, nphi, ntheta, nshift, &grid);
   if (!st) st = ws_get(ctx, WS_IN, sizeof(double) * nin, &din);
   if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
-  if (!st) st = h2d(ctx, din, rays, sizeof(double) * nin, "reduction input");
+  if (!st) st = h2d_staged(ctx, din, rays, sizeof(double) * nin, "reduction input");
   if (!st)
     st = wrt_radon_reduction_device(ctx, static_cast<const double *>(din), ngrid, nshift_ray, grid,
                                     static_cast<double *>(dout));
-  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "reduction result");
+  if (!st) st = d2h_staged_sync(ctx, out, dout, sizeof(double) * nout, "reduction result");
   return st;
 }
 
@@ -1064,11 +1068,11 @@ int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
   st = dropin_grid(ctx, nphi, ntheta, nshift, &grid);
   if (!st) st = ws_get(ctx, WS_IN, sizeof(double) * nin, &din);
   if (!st) st = ws_get(ctx, WS_OUT, sizeof(double) * nout, &dout);
-  if (!st) st = h2d(ctx, din, radon, sizeof(double) * nin, "adjoint input");
+  if (!st) st = h2d_staged(ctx, din, radon, sizeof(double) * nin, "adjoint input");
   if (!st)
     st = wrt_radon3d_adjoint_device(ctx, static_cast<const double *>(din), grid, ngrid,
                                     static_cast<double *>(dout));
-  if (!st) st = d2h_sync(ctx, out, dout, sizeof(double) * nout, "adjoint result");
+  if (!st) st = d2h_staged_sync(ctx, out, dout, sizeof(double) * nout, "adjoint result");
   return st;
 }
 

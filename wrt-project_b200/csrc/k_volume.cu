@@ -134,11 +134,6 @@ int convert(wrt_ctx *ctx, const T *d_src, int n, float *d_vol, unsigned int *d_s
 
 namespace wrt {
 
-int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
-                    unsigned int *d_r2bits) {
-  return convert(ctx, d_src, n, d_vol, d_r2bits);
-}
-
 int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
                     unsigned int *d_r2bits) {
   return convert(ctx, d_src, n, d_vol, d_r2bits);

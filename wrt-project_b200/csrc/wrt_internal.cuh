@@ -34,6 +34,10 @@
 #define WRT_PI 3.14159265358979323846
 
 // ---------------------------------------------------------------- host side
+namespace wrt {
+struct HostPool;  // host threads of the staged copies (hostcopy.cu)
+}
+
 struct wrt_ctx {
   int device = 0;
   size_t budget = 0;      // 0 = unlimited
@@ -65,6 +69,12 @@ struct wrt_ctx {
   // for the next call of the same sizes
   wrt_volume *dropin_vol = nullptr;
   wrt_grid *dropin_grid = nullptr;
+  // host-array copies (hostcopy.cu): two pinned chunk buffers, the events
+  // that end their DMA, and the host threads that fill and drain them
+  void *pin[2] = {};
+  cudaEvent_t pin_ev[2] = {};
+  wrt::HostPool *host_pool = nullptr;
+  unsigned long long large_copies = 0;  // host-array copies of 1 MB or more so far
 };
 
 namespace wrt {
@@ -79,6 +89,17 @@ int check_launch(wrt_ctx *ctx, const char *what);
 // stream has drained; contents are not kept).
 enum WsRole { WS_STAGE, WS_IN, WS_OUT, WS_LINES, WS_SPLINE, WS_COEF, WS_TABLE, WS_FFT, WS_ROLES };
 int ws_get(wrt_ctx *ctx, int role, size_t bytes, void **p);
+// Copies between caller (pageable) host arrays and the device, through the
+// context's pinned chunk buffers and host threads (hostcopy.cu): the upload
+// returns once the caller's array has been read (the DMA may still run, in
+// stream order); the download returns with the data in place.
+int h2d_staged(wrt_ctx *ctx, void *dst, const void *src, size_t bytes, const char *what);
+// FP64 host values rounded to FP32 (to nearest) while they are staged.
+int h2d_staged_rounded(wrt_ctx *ctx, float *dst, const double *src, size_t count,
+                       const char *what);
+int d2h_staged_sync(wrt_ctx *ctx, void *dst, const void *src, size_t bytes, const char *what);
+void pinned_release(wrt_ctx *ctx);
+void host_pool_destroy(HostPool *p);
 
 // Host-side FP64 geometry, computed with the host libm exactly as the
 // reference computes it (radon_grid/src/integral.c:10-36).
@@ -97,8 +118,6 @@ void adjoint_directions(int nphi, int ntheta, int nshift, const double *phi, con
 
 // Volume preparation kernels (k_volume.cu).
 // d_stats[0]: largest |x|^2 of a non-zero node, d_stats[1]: max |v| (float bits)
-int volume_from_f64(wrt_ctx *ctx, const double *d_src, int n, float *d_vol,
-                    unsigned int *d_stats);
 int volume_from_f32(wrt_ctx *ctx, const float *d_src, int n, float *d_vol,
                     unsigned int *d_stats);
 int volume_pairs(wrt_ctx *ctx, const float *d_vol, int n, float2 *d_pairs, int pitch);
