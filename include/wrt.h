@@ -321,7 +321,9 @@ int wrt_device_alloc(wrt_ctx *ctx, size_t bytes, void **dev_ptr);
 int wrt_device_free(wrt_ctx *ctx, void *dev_ptr);
 int wrt_host_alloc_pinned(wrt_ctx *ctx, size_t bytes, void **host_ptr);
 int wrt_host_free_pinned(wrt_ctx *ctx, void *host_ptr);
-/* Copies ordered on the context's stream; the device-to-host copy waits. */
+/* Copies ordered on the context's stream; the host array may be pageable.
+ * The host-to-device copy returns once the host array has been read (the
+ * transfer completes in stream order); the device-to-host copy waits. */
 int wrt_copy_to_device(wrt_ctx *ctx, void *dev_dst, const void *host_src, size_t bytes);
 int wrt_copy_to_host(wrt_ctx *ctx, void *host_dst, const void *dev_src, size_t bytes);
 

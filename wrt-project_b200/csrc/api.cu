@@ -389,7 +389,7 @@ int wrt_host_free_pinned(wrt_ctx *ctx, void *host_ptr) {
 
 int wrt_copy_to_device(wrt_ctx *ctx, void *dst, const void *src, size_t bytes) {
   if (!ctx || !dst || !src) return WRT_ERR_INVALID_ARGUMENT;
-  return h2d(ctx, dst, src, bytes, "copy to device");
+  return h2d_staged(ctx, dst, src, bytes, "copy to device");
 }
 
 int wrt_copy_to_host(wrt_ctx *ctx, void *dst, const void *src, size_t bytes) {
