@@ -232,7 +232,8 @@ __global__ void __launch_bounds__(256) batch_reduction_kernel(const char *t) {
   for (int r = 0; r < nr; ++r) {
     const RedReq &q = Q[r];
     const long long total = (long long)q.nshift * q.nphi * q.ntheta;
-    for (long long k = dealt_first(tid, first, nth); k < total; k += nth) {
+    for (long long t = dealt_first(tid, first, nth); t < total; t += nth) {
+      const long long k = wrtd::reduction_sample_of(t, q.nshift, q.nphi, q.ntheta);
       int evaluated = 0;
       q.out[k] = wrtd::reduction_one(q.lines, q.ngrid, q.ns_ray, q.nphi, q.shift, q.cs, q.ntheta, k,
                                      &evaluated);

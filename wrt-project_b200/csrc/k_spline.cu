@@ -42,14 +42,16 @@ __global__ void spline_prep_kernel(const double *__restrict__ src, int nlines, i
                       out + (size_t)L * (ns - 1));
 }
 
-// Reduction: one thread per Radon sample (wrtd::reduction_one).
+// Reduction: one thread per Radon sample (wrtd::reduction_one), a warp on
+// consecutive shifts (wrtd::reduction_sample_of).
 __global__ void __launch_bounds__(256)
     reduction_kernel(const float4 *__restrict__ lines /* [iz][iphi][ns_ray-1] */, int ngrid,
                      int ns_ray, int nphi, const double *__restrict__ shift, int nshift,
                      const double *__restrict__ cs /* [ntheta][2] cos, sin */, int ntheta,
                      double *__restrict__ out, unsigned long long *counter) {
-  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= (long long)nshift * nphi * ntheta) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nshift * nphi * ntheta) return;
+  const long long k = wrtd::reduction_sample_of(t, nshift, nphi, ntheta);
   int evaluated = 0;
   out[k] = wrtd::reduction_one(lines, ngrid, ns_ray, nphi, shift, cs, ntheta, k, &evaluated);
   if (counter) atomicAdd(counter, (unsigned long long)evaluated);

@@ -86,6 +86,17 @@ __device__ __forceinline__ float cubic_centred(const float4 c, float u) {
 }
 
 // ------------------------------------------------------------ reduction
+// The Radon sample that thread t of a reduction computes: threads run over
+// the shifts fastest, so a warp's 32 samples share (iphi, itheta) and their
+// slices lie side by side (neighbouring spline records of the same layers);
+// the output keeps the reference's order (is, iphi, itheta).
+__host__ __device__ inline long long reduction_sample_of(long long t, int nshift, int nphi,
+                                                         int ntheta) {
+  const long long is = t % nshift, r = t / nshift;
+  const long long it = r % ntheta, ip = r / ntheta;
+  return (is * nphi + ip) * ntheta + it;
+}
+
 // radon_reduction (radon_reduction/slicing.c:80-119) of Radon sample k
 // (is, iphi, itheta), order of reduction.c:215-229, from the reduction lines
 // [iz][iphi][ns_ray-1] of the ray data, by one thread: geometry in FP64 with
