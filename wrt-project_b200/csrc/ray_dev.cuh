@@ -7,9 +7,8 @@
 // sampler.  With a frame F every point is mapped to F p(k) (the layer scheme
 // about another axis; F = identity reproduces the reference).
 //
-// One lane per ray; a warp takes 32 consecutive shifts of one (z, phi):
-// parallel rays one shift step apart, whose samples read neighbouring cache
-// lines (2.2x faster than 32 angles of one shift, which fan out).  Samples
+// One lane per ray; the kernels choose which rays share a warp (k_ray.cu: a
+// tile of consecutive shifts x consecutive angles of one layer).  Samples
 // farther than sqrt(crop_r2) from the origin or outside the cube are skipped
 // (their value is exactly 0).  Numerics: FP32 cell coordinates with the guard
 // band of wrt_internal.cuh.  In the reference frame the z coordinate of a ray
