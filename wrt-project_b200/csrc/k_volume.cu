@@ -49,12 +49,13 @@ __global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *_
   }
 }
 
-// oct[2c], oct[2c+1]: corners of cell c = (ix*(n-1) + iy)*(n-1) + iz.
+// oct[2c], oct[2c+1]: corners of cell c = (iz*(n-1) + iy)*(n-1) + ix (x
+// fastest: the cells a layer's rays cross side by side are neighbours).
 __global__ void volume_octets_kernel(const float *__restrict__ v, int n, float4 *__restrict__ oct) {
   const size_t m = (size_t)(n - 1), total = m * m * m;
   for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total;
        c += (size_t)gridDim.x * blockDim.x) {
-    const int iz = (int)(c % m), iy = (int)((c / m) % m), ix = (int)(c / (m * m));
+    const int ix = (int)(c % m), iy = (int)((c / m) % m), iz = (int)(c / (m * m));
     const float *q = v + ((size_t)ix * n + iy) * n + iz;
     const size_t sx = (size_t)n * n;
     oct[2 * c] = make_float4(q[0], q[1], q[n], q[n + 1]);

@@ -209,7 +209,7 @@ __device__ __forceinline__ void ray_one(const wrt::RayJob &job, long long ray, f
     auto gather = [&](const RayCell &c, float4 &lo, float4 &hi) {
       const unsigned ix = c.bx - mb, iy = c.by - mb, izc = c.bz - mb;
       if (job.oct) {
-        ld_octet(job.oct, ((size_t)ix * (n - 1) + iy) * (n - 1) + izc, lo, hi);
+        ld_octet(job.oct, ((size_t)izc * (n - 1) + iy) * (n - 1) + ix, lo, hi);
       } else if (!FRAME && job.pairs) {
         // one z-layer pair: rows contiguous in x
         const float2 *p = job.pairs + ((size_t)izc * n + iy) * job.pitch + ix;
