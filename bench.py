@@ -434,6 +434,73 @@ def other_paths(wrt, ctx, phantom, steps, warmup, smem_bw, with_cpu):
     return res
 
 
+def config_runs(wrt, ctx, steps):
+    """The ray and 256^3 configurations at their stated sizes through the
+    device-resident entry points (device time, CUDA events on the library's
+    stream, L2 flushed before each timed call): the ray transform in 64 layer
+    orientations (the reference frame and 63 seeded rotations) x 128 layers x
+    128 shifts x 128 angles at 128^3 followed by the reduction of the reference
+    frame's rays to a 64x128 sphere grid x 256 shifts; the forward transform
+    of a 256^3 volume (16 seeded ellipsoids) in FP32 and in BF16 storage on a
+    96x192 sphere grid x 384 shifts (trilinear, lattice [-n, n)^2); and the
+    backprojection of seeded N(0,1) Radon data on that grid back to 256^3."""
+    from wrt_b200.phantom import ellipsoid_phantom, layer_frames
+
+    res = {}
+    n = 128
+    vol = wrt.Volume(ctx, n)
+    vol.upload(ellipsoid_phantom(n, ELLIPSOIDS, SEED).astype(np.float32))
+    frames = layer_frames(64, 1101)
+    nrays = n * RAY_SHIFTS * RAY_PHIS
+    rays0 = wrt.DeviceBuffer(ctx, nrays * 8)
+    rays = wrt.DeviceBuffer(ctx, nrays * 8)
+    grid = wrt.Grid(ctx, NPHI, NTHETA, NSHIFT)
+    radon = wrt.DeviceBuffer(ctx, grid.nplanes * 8)
+
+    def rays_and_reduction():
+        for k, F in enumerate(frames):
+            wrt.ray_forward_device(ctx, vol, n, RAY_SHIFTS, RAY_PHIS,
+                                   (rays0 if k == 0 else rays).ptr, frame=None if k == 0 else F)
+        wrt.radon_reduction_device(ctx, rays0.ptr, n, RAY_SHIFTS, grid, radon.ptr)
+    t = statistics.mean(timed_device_calls(ctx, rays_and_reduction, steps, 1))
+    res["rays_64_orientations_and_reduction_128"] = {
+        "ms": t, "rays_per_s": 64 * nrays / (t * 1e-3),
+        "workload": "128^3: ray transform in 64 layer orientations x 128 layers x 128 shifts x "
+                    "128 angles, then the reduction of orientation 0 to 64x128 x 256 shifts"}
+    for b in (rays0, rays, radon):
+        b.close()
+    grid.close()
+    vol.close()
+
+    n3, nphi, ntheta, nshift = 256, 192, 96, 384
+    phantom = ellipsoid_phantom(n3, ELLIPSOIDS, 1003)
+    grid3 = wrt.Grid(ctx, nphi, ntheta, nshift)
+    out3 = wrt.DeviceBuffer(ctx, grid3.nplanes * 8)
+    for storage, name in ((wrt.STORAGE_F32, "forward_256_f32"),
+                          (wrt.STORAGE_BF16, "forward_256_bf16")):
+        v = wrt.Volume(ctx, n3, storage=storage)
+        v.upload(phantom)
+        t = statistics.mean(timed_device_calls(
+            ctx, lambda: wrt.radon_forward_batch(ctx, [(v, grid3, out3.ptr, n3)]), steps, 1))
+        res[name] = {"ms": t, "plane_integrals_per_s": grid3.nplanes / (t * 1e-3),
+                     "workload": f"256^3 ({'FP32' if storage == wrt.STORAGE_F32 else 'BF16'} "
+                                 "storage), 96x192 sphere grid x 384 shifts, trilinear, "
+                                 "lattice [-n, n)^2"}
+        v.close()
+    g = np.random.default_rng(4004).standard_normal((nshift, nphi, ntheta))
+    out3.upload(g)
+    adj = wrt.DeviceBuffer(ctx, n3 ** 3 * 8)
+    t = statistics.mean(timed_device_calls(
+        ctx, lambda: wrt.radon3d_adjoint_device(ctx, out3.ptr, grid3, n3, adj.ptr), steps, 1))
+    res["adjoint_256"] = {"ms": t, "voxels_per_s": n3 ** 3 / (t * 1e-3),
+                          "spline_evaluations_per_s": n3 ** 3 * nphi * ntheta / (t * 1e-3),
+                          "workload": "N(0,1) Radon data 96x192 x 384 shifts -> 256^3 voxels"}
+    adj.close()
+    out3.close()
+    grid3.close()
+    return res
+
+
 def batch_vs_one_per_launch(wrt, ctx, steps, count=64, edges=(48, 64, 96, 128, 160, 192),
                             lat=(16, 97), shifts=(64, 257), seed=2002):
     """`count` FP32 volumes of uneven edge lengths (drawn from `edges`), each
@@ -802,7 +869,8 @@ def run_ours(args, dist):
     grid = wrt.Grid(ctx, NPHI, NTHETA, NSHIFT)
     nplanes = grid.nplanes
     out = wrt.DeviceBuffer(ctx, nplanes * 8)
-    kernel = {"plain": wrt.KERNEL_PLAIN, "staged": wrt.KERNEL_STAGED, "auto": wrt.KERNEL_AUTO}[args.kernel]
+    kernel = {"plain": wrt.KERNEL_PLAIN, "staged": wrt.KERNEL_STAGED,
+              "auto": wrt.KERNEL_AUTO}[args.kernel]
 
     def step(k=kernel):
         if k == wrt.KERNEL_PLAIN:
@@ -951,6 +1019,7 @@ def run_ours(args, dist):
         result["batch_vs_one_per_launch_small"] = batch_vs_one_per_launch(
             wrt, ctx, 3, count=256, edges=(16, 24, 32, 48), lat=(8, 17), shifts=(32, 65),
             seed=2003)
+        result["configs"] = config_runs(wrt, ctx, 2)
     if dist.rank == 0 and dist.world == 1 and not args.no_serving_mix:
         result["serving"] = serving_mix(wrt, dev, args.mix_requests, 4000, 60 << 30)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
