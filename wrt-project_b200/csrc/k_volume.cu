@@ -51,11 +51,14 @@ __global__ void volume_convert_kernel(const T *__restrict__ src, int n, float *_
 
 // oct[2c], oct[2c+1]: corners of cell c = (iz*(n-1) + iy)*(n-1) + ix (x
 // fastest: the cells a layer's rays cross side by side are neighbours).
+// Threads run over z fastest, so the volume reads coalesce; each thread
+// writes its cell's whole 32-byte sector.
 __global__ void volume_octets_kernel(const float *__restrict__ v, int n, float4 *__restrict__ oct) {
   const size_t m = (size_t)(n - 1), total = m * m * m;
-  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < total;
-       c += (size_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(c % m), iy = (int)((c / m) % m), iz = (int)(c / (m * m));
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const int iz = (int)(k % m), iy = (int)((k / m) % m), ix = (int)(k / (m * m));
+    const size_t c = ((size_t)iz * m + iy) * m + ix;
     const float *q = v + ((size_t)ix * n + iy) * n + iz;
     const size_t sx = (size_t)n * n;
     oct[2 * c] = make_float4(q[0], q[1], q[n], q[n + 1]);
