@@ -348,6 +348,21 @@ def other_paths(wrt, ctx, phantom, steps, warmup, smem_bw, with_cpu):
                  ("reduction", "128^3 rays (128 offsets) -> 64x128 sphere grid x 256 shifts"),
                  ("adjoint", "N(0,1) Radon data 64x128x256 -> 128^3 voxels")):
         res[k]["workload"] = w
+    # what binds each kernel, from its committed ncu capture (a profiler cannot
+    # run inside the timed bench): the byte figure above is the algorithmic
+    # gather, not always the limit
+    for k, b in (("nearest", "issue: 79 % of issue slots, 3.15 instructions per clock; a 4-byte "
+                             "warp load is one shared wavefront, so the byte figure is not the "
+                             "limit (profiles/plane_staged_nearest_128cubed.md)"),
+                 ("ray", "L1 gathers: 64 % of L1 throughput, 20 of 32 lanes busy (parallel rays "
+                         "of different chord lengths) (profiles/ray_kernel_128cubed.md)"),
+                 ("ray_rotated", "L1 gathers: 82 % of L1 throughput "
+                                 "(profiles/ray_kernel_128cubed.md)"),
+                 ("reduction", "L1 sectors: 97.5 % of L1 throughput at ~30 sectors per request "
+                               "(profiles/reduction_kernel_128cubed.md)"),
+                 ("adjoint", "latency of the record gathers: long-scoreboard stalls, 68 % issue, "
+                             "59 % of the L1 data pipe (profiles/adjoint_kernel_128cubed.md)")):
+        res[k]["roofline"]["limit_measured"] = b
     if with_cpu:
         import oracle as O
         cores = cpu_threads()
