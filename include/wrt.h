@@ -58,10 +58,12 @@ typedef enum wrt_sampler {
 } wrt_sampler;
 
 typedef enum wrt_kernel {
-  WRT_KERNEL_AUTO = 0,   /* trilinear: the staged kernel when it applies; nearest: rows
-                            walked by whole warps over a z-major copy of the volume */
+  WRT_KERNEL_AUTO = 0,   /* the staged kernel (both samplers; volumes of edge >= 4),
+                            else the plain one */
   WRT_KERNEL_PLAIN = 1,  /* one warp per plane, gathers through L1 */
-  WRT_KERNEL_STAGED = 2  /* volume layers staged in shared memory, persistent CTAs */
+  WRT_KERNEL_STAGED = 2  /* volume layers staged in shared memory, persistent CTAs:
+                            trilinear from the layer pairs (FP32 or BF16 storage),
+                            nearest from the z-major cell layers (FP32 storage) */
 } wrt_kernel;
 
 /* Options of the plane-integral transform.  Zero-initialised options give the
