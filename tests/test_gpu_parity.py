@@ -173,6 +173,27 @@ def test_staged_nearest_matches_oracle_and_plain(ctx, n, grid, L):
     assert rel_l2(got, plain) < 1e-6
 
 
+@pytest.mark.parametrize("sampler,L", [(O.NEAREST, 72), (O.TRILINEAR, 96)])
+def test_staged_lattice_beyond_the_reference_extent(ctx, vol24, sampler, L):
+    """Lattices wider than the reference's [-2n, 2n)^2 (up to 8n is accepted):
+    the rows leave the cube further out, the row indices still fit the tables."""
+    got = ctx.radon_grid(vol24, 8, 4, 6, sampler=sampler, half_extent=L,
+                         kernel=wrt.KERNEL_STAGED)
+    ref = O.radon_forward(vol24, 8, 4, 6, sampler=sampler, half_extent=L)
+    assert rel_l2(got, ref) < TOL_L2
+
+
+def test_ray_tiles_at_ragged_grid_sizes(ctx, vol24):
+    """Shift and angle counts that are not multiples of a warp's tile (16 x 2
+    in the reference frame, 2 x 16 in rotated ones)."""
+    F = layer_frames(2, 77)[1]
+    for nshift, nphi in ((15, 17), (33, 3), (2, 1)):
+        for fr in (None, F):
+            got = ctx.ray_grid(vol24, 24, nshift, nphi, frame=fr)
+            ref = O.ray_forward(vol24, 24, nshift, nphi, frame=fr)
+            assert rel_l2(got, ref) < TOL_L2, (nshift, nphi, fr is None)
+
+
 def test_staged_nearest_random_volume_nonzero_faces(ctx, volrand):
     got = ctx.radon_grid(volrand, 8, 6, 9, sampler=O.NEAREST, kernel=wrt.KERNEL_STAGED)
     ref = O.radon_forward(volrand, 8, 6, 9, sampler=O.NEAREST)
