@@ -1,10 +1,14 @@
 /* CPU check of the drop-in programs' parallel text reader (cli/cli_common.c):
  * files of "%lf" lines and "%lf, %lf, %lf, %lf" lines are read with 1, 3, 8
  * and 16 threads and must give exactly the values of a serial strtod parse;
- * a truncated file and a malformed line must be refused. */
+ * a truncated file and a malformed line must be refused; a FIFO (a stream
+ * that cannot seek) must read like the file it carries. */
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
+#include <sys/wait.h>
+#include <unistd.h>
 
 #include "cli_common.h"
 
@@ -52,6 +56,32 @@ int main(int argc, char **argv) {
         printf("FAIL prefix read\n");
         return 1;
       }
+    }
+    /* the same text through a FIFO, written by a child process */
+    char fifo[4096];
+    snprintf(fifo, sizeof fifo, "%s/fifo_%d", dir, columns);
+    unlink(fifo);
+    if (mkfifo(fifo, 0600) != 0) {
+      printf("FAIL mkfifo\n");
+      return 1;
+    }
+    pid_t child = fork();
+    if (child == 0) {
+      FILE *src = fopen(path, "rb"), *dst = fopen(fifo, "wb");
+      char chunk[1 << 16];
+      size_t m;
+      while (src && dst && (m = fread(chunk, 1, sizeof chunk, src)) > 0) fwrite(chunk, 1, m, dst);
+      const int ok = src && dst && fclose(dst) == 0; /* _exit flushes no stdio buffer */
+      _exit(ok ? 0 : 1);
+    }
+    memset(got, 0, n * sizeof(double));
+    int frc = columns == 1 ? cli_read_column(fifo, n, got, 8) : cli_read_csv4(fifo, n, got, 8);
+    int status = 0;
+    waitpid(child, &status, 0);
+    unlink(fifo);
+    if (frc || memcmp(got, want, n * sizeof(double)) || !WIFEXITED(status) || WEXITSTATUS(status)) {
+      printf("FAIL fifo columns=%d rc=%d\n", columns, frc);
+      return 1;
     }
     /* more values than the file holds: refused */
     if ((columns == 1 ? cli_read_column(path, n + 1, got, 8) : cli_read_csv4(path, n + 1, got, 8)) == 0) {

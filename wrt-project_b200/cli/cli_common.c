@@ -113,6 +113,34 @@ int cli_read_params(const char *path, int p[4]) {
   return 0;
 }
 
+/* A stream that cannot seek (a pipe, a FIFO, /dev/stdin: the reference's
+ * "%lf" loop reads those too), read to its end into a growing buffer. */
+static char *slurp_stream(FILE *f, size_t *len) {
+  size_t cap = (size_t)1 << 20, n = 0;
+  char *buf = malloc(cap + 1);
+  while (buf) {
+    n += fread(buf + n, 1, cap - n, f);
+    if (n < cap) break; /* end of stream or a read error */
+    char *nb = realloc(buf, 2 * cap + 1);
+    if (!nb) {
+      free(buf);
+      buf = NULL;
+      break;
+    }
+    buf = nb;
+    cap *= 2;
+  }
+  if (buf && ferror(f)) {
+    free(buf);
+    buf = NULL;
+  }
+  if (buf) {
+    buf[n] = 0;
+    *len = n;
+  }
+  return buf;
+}
+
 /* Whole-file read; returns a NUL-terminated buffer or NULL. */
 static char *slurp(const char *path, size_t *len) {
   FILE *f = fopen(path, "rb");
@@ -120,19 +148,26 @@ static char *slurp(const char *path, size_t *len) {
     fprintf(stderr, "Recieved call %s while opening %s. \n", strerror(errno), path);
     return NULL;
   }
-  fseek(f, 0, SEEK_END);
-  long n = ftell(f);
-  fseek(f, 0, SEEK_SET);
-  char *buf = malloc((size_t)n + 1);
-  if (!buf || fread(buf, 1, (size_t)n, f) != (size_t)n) {
-    fprintf(stderr, "Error: could not read %s\n", path);
-    free(buf);
-    fclose(f);
-    return NULL;
+  long n = -1;
+  if (fseek(f, 0, SEEK_END) == 0) {
+    n = ftell(f);
+    if (fseek(f, 0, SEEK_SET) != 0) n = -1;
   }
-  buf[n] = 0;
+  char *buf = NULL;
+  if (n < 0) {
+    buf = slurp_stream(f, len);
+  } else {
+    buf = malloc((size_t)n + 1);
+    if (buf && fread(buf, 1, (size_t)n, f) == (size_t)n) {
+      buf[n] = 0;
+      *len = (size_t)n;
+    } else {
+      free(buf);
+      buf = NULL;
+    }
+  }
+  if (!buf) fprintf(stderr, "Error: could not read %s\n", path);
   fclose(f);
-  *len = (size_t)n;
   return buf;
 }
 
