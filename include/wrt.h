@@ -139,7 +139,7 @@ int wrt_radon3d_adjoint(wrt_ctx *ctx, const double *radon, int nphi, int ntheta,
  * after start-up (cudaMalloc/cudaFree synchronise the device).  d_radon
  * (nshift*nphi*ntheta doubles, order [is][iphi][itheta]) and d_out (ngrid^3
  * doubles, order [iz][ix][iy]) are device buffers owned by the caller; the
- * working memory is one fixed ~6.6 MB array inside the library, held by every
+ * working memory is one fixed ~6.8 MB array inside the library, held by every
  * GPU that loads the library until the process exits.  Limits: nphi*ntheta
  * <= 16384, ntheta <= 1024, 3 <= nshift <= 2048, nphi*ntheta*nshift <=
  * 262144; larger sizes return WRT_ERR_INVALID_ARGUMENT with a message.  The

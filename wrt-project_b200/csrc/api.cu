@@ -913,7 +913,8 @@ int wrt_radon_grid(wrt_ctx *ctx, const double *volume, int n, int nphi, int nthe
 int wrt_radon_transpose(wrt_ctx *ctx, const double *g, int n, int nphi, int ntheta, int nshift,
                         const wrt_plane_opts *opts, double *out_volume) {
   if (!ctx || !g || !out_volume || n < 2 || nphi < 1 || ntheta < 1 || nshift < 2)
-    return WRT_ERR_INVALID_ARGUMENT;
+    return ctx ? fail(ctx, WRT_ERR_INVALID_ARGUMENT, "radon_transpose: bad arguments")
+               : WRT_ERR_INVALID_ARGUMENT;
   if (!valid_plane_opts(opts, n)) return fail(ctx, WRT_ERR_INVALID_ARGUMENT, "invalid plane options");
   wrt_plane_opts o = {};
   if (opts) o = *opts;

@@ -136,9 +136,14 @@ extern "C" int wrt_fourier_slice_inversion(wrt_ctx *ctx, const double *radon, in
   if (e != cudaSuccess) return wrt::cuda_fail(ctx, e, "cudaSetDevice");
   // the reference's discretisation (rtft3d.m:41-46)
   const double ds = 2.0 * rsupp / (nshift - 1);
-  const int ntotal = padding * (int)floor(1.0 / ds);
-  if (ntotal < 2)
+  // the frequency count in FP64 first: a tiny rsupp would overflow the int
+  const double nfreq = padding * floor(1.0 / ds);
+  if (!(nfreq >= 2.0))
     return wrt::fail(ctx, WRT_ERR_INVALID_ARGUMENT, "fourier_slice_inversion: too few frequencies");
+  if (nfreq > (double)(1 << 24))
+    return wrt::fail(ctx, WRT_ERR_INVALID_ARGUMENT,
+                     "fourier_slice_inversion: %.0f padded shifts (at most %d)", nfreq, 1 << 24);
+  const int ntotal = (int)nfreq;
   const double dnu = 1.0 / (ntotal * ds);
   const int K = ntotal / 2, ndir = nphi * ntheta;
   // sphere grid (GL nodes on the GPU) and per-direction weights / unit vectors
