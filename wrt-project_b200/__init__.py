@@ -201,6 +201,28 @@ def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def _cube(a, dtype=np.float64) -> np.ndarray:
+    """A C-contiguous n x n x n volume; anything else raises ValueError (the
+    library reads n^3 values from the pointer it is given)."""
+    v = np.ascontiguousarray(a, dtype=dtype)
+    if v.ndim != 3 or not v.shape[0] == v.shape[1] == v.shape[2]:
+        raise ValueError(f"volume must be an n x n x n array, got shape {v.shape}")
+    return v
+
+
+def _require(cond: bool, message: str):
+    """Argument check that stays on under ``python -O`` (unlike assert): a
+    wrong size here would let the library read or write past a buffer."""
+    if not cond:
+        raise ValueError(message)
+
+
+def _out_array(out, count: int, what: str):
+    _require(isinstance(out, np.ndarray) and out.flags.c_contiguous and out.dtype == np.float64
+             and out.size == count, f"{what}: out must be a C-contiguous float64 array of "
+                                    f"{count} values")
+
+
 def plane_opts(sampler=NEAREST, half_extent=0, kernel=KERNEL_AUTO) -> PlaneOpts:
     o = PlaneOpts()
     o.sampler, o.half_extent, o.kernel = int(sampler), int(half_extent or 0), int(kernel)
@@ -303,7 +325,7 @@ class Context:
     # -- drop-in transforms
     def radon_grid(self, volume, nphi, ntheta, nshift, sampler=NEAREST, half_extent=0,
                    kernel=KERNEL_AUTO) -> np.ndarray:
-        v = _f64(volume)
+        v = _cube(volume)
         n = v.shape[0]
         out = np.empty((nshift, nphi, ntheta))
         o = plane_opts(sampler, half_extent, kernel)
@@ -312,7 +334,7 @@ class Context:
         return out
 
     def ray_grid(self, volume, nslices, nshift, nphi, frame=None) -> np.ndarray:
-        v = _f64(volume)
+        v = _cube(volume)
         out = np.empty((nslices, nshift, nphi))
         f = None if frame is None else _f64(frame).reshape(9)
         fp = None if f is None else f.ctypes.data_as(_vp)
@@ -366,9 +388,8 @@ class Context:
     def spectral_laplacian(self, volume, period=2.0) -> np.ndarray:
         """ifftn(-(2 pi/period)^2 |k|^2 fftn(volume)) of an n^3 array
         (laplace3dfft.m), FP64 FFTs on the device."""
-        v = _f64(volume)
+        v = _cube(volume)
         n = v.shape[0]
-        assert v.shape == (n, n, n)
         out = np.empty_like(v)
         self.check(lib().wrt_spectral_laplacian(self._h, v, n, float(period), out),
                    "spectral_laplacian")
@@ -405,12 +426,13 @@ class DeviceBuffer:
 
     def upload(self, host: np.ndarray):
         a = np.ascontiguousarray(host)
-        assert a.nbytes <= self.nbytes
+        _require(a.nbytes <= self.nbytes, f"upload of {a.nbytes} bytes into a {self.nbytes}-byte buffer")
         self.ctx.check(lib().wrt_copy_to_device(self.ctx.handle, self._p, a.ctypes.data_as(_vp),
                                                 a.nbytes), "copy_to_device")
 
     def download(self, out: np.ndarray) -> np.ndarray:
-        assert out.flags.c_contiguous and out.nbytes <= self.nbytes
+        _require(isinstance(out, np.ndarray) and out.flags.c_contiguous and out.nbytes <= self.nbytes,
+                 f"download needs a C-contiguous array of at most {self.nbytes} bytes")
         self.ctx.check(lib().wrt_copy_to_host(self.ctx.handle, out.ctypes.data_as(_vp), self._p,
                                               out.nbytes), "copy_to_host")
         return out
@@ -625,9 +647,8 @@ class Server:
 
     def submit_forward(self, volume, nphi, ntheta, nshift, out, half_extent=0, tag=0) -> int:
         """volume: float32 [n][n][n]; out: float64 [nshift][nphi][ntheta]."""
-        v = np.ascontiguousarray(volume, dtype=np.float32)
-        assert out.flags.c_contiguous and out.dtype == np.float64
-        assert out.size == nshift * nphi * ntheta
+        v = _cube(volume, np.float32)
+        _out_array(out, nshift * nphi * ntheta, "submit_forward")
         r = Request(OP_FORWARD, v.shape[0], nphi, ntheta, nshift, int(half_extent),
                     v.ctypes.data, None, out.ctypes.data, int(tag))
         return self._submit(r, (v, out))
@@ -635,8 +656,9 @@ class Server:
     def submit_adjoint(self, radon, ngrid, out, tag=0) -> int:
         """radon: float64 [nshift][nphi][ntheta]; out: float64 [n][n][n] ([iz][ix][iy])."""
         g = np.ascontiguousarray(radon, dtype=np.float64)
+        _require(g.ndim == 3, f"radon data must be [nshift][nphi][ntheta], got shape {g.shape}")
         nshift, nphi, ntheta = g.shape
-        assert out.flags.c_contiguous and out.dtype == np.float64 and out.size == ngrid ** 3
+        _out_array(out, int(ngrid) ** 3, "submit_adjoint")
         r = Request(OP_ADJOINT, int(ngrid), nphi, ntheta, nshift, 0, None, g.ctypes.data,
                     out.ctypes.data, int(tag))
         return self._submit(r, (g, out))
@@ -644,9 +666,8 @@ class Server:
     def submit_ray(self, volume, nslices, nshift, nphi, out, frame=None, tag=0) -> int:
         """volume: float32 [n][n][n]; out: float64 [nslices][nshift][nphi]
         (ray_grid's order); frame: None (z-slices) or a 3x3 rotation."""
-        v = np.ascontiguousarray(volume, dtype=np.float32)
-        assert out.flags.c_contiguous and out.dtype == np.float64
-        assert out.size == nslices * nshift * nphi
+        v = _cube(volume, np.float32)
+        _out_array(out, nslices * nshift * nphi, "submit_ray")
         f = None if frame is None else _f64(frame).reshape(9)
         r = Request(op=OP_RAY, ngrid=v.shape[0], nphi=int(nphi), ntheta=1, nshift=int(nshift),
                     volume=v.ctypes.data, out=out.ctypes.data, tag=int(tag),
@@ -657,9 +678,9 @@ class Server:
         """rays: float64 [ngrid][nshift_ray][nphi]; out: float64
         [nshift][nphi][ntheta] on the Gauss-uniform sphere grid."""
         g = np.ascontiguousarray(rays, dtype=np.float64)
+        _require(g.ndim == 3, f"ray data must be [ngrid][nshift_ray][nphi], got shape {g.shape}")
         ngrid, nsr, nphi = g.shape
-        assert out.flags.c_contiguous and out.dtype == np.float64
-        assert out.size == nshift * nphi * ntheta
+        _out_array(out, nshift * nphi * ntheta, "submit_reduce")
         r = Request(op=OP_REDUCE, ngrid=ngrid, nphi=nphi, ntheta=int(ntheta), nshift=int(nshift),
                     out=out.ctypes.data, tag=int(tag), nshift_ray=nsr, rays=g.ctypes.data)
         return self._submit(r, (g, out))
