@@ -2,7 +2,7 @@
  * Radon / ray transform hot path.
  *
  * TEST INFRASTRUCTURE ONLY.  This is the checker: the tests, the smoke check
- * and the benchmark's CPU-baseline leg call it to judge the CUDA library.  The
+ * and the benchmark's CPU-baseline leg call it to check the CUDA library.  The
  * product (libwrt.so and the drop-in programs) never links or calls it.
  *
  * Every function restates one reference function, keeping its arithmetic in
