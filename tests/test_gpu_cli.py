@@ -1,9 +1,10 @@
-"""Drop-in contract: the four programs against the reference's own programs
+"""Drop-in contract: the programs against the reference's own programs
 (compiled from the reference sources into oracle/_ref) on the same parameter
 and data files.  Same argv, same file formats, same row order; values agree
 to the printed precision ("%lf", 6 decimals) and readme_<OUT> is identical
 (radon_grid, ray_grid and the adjoint; radon_reduction differs only where the
-reference prints nothing different)."""
+reference prints nothing different).  The analytic programs are in
+test_gpu_zz_analytic_programs.py."""
 import shutil
 import subprocess
 from pathlib import Path

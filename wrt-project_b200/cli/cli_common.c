@@ -17,43 +17,60 @@ double cli_now(void) {
   return t.tv_sec + 1e-9 * t.tv_nsec;
 }
 
-static void usage_exit(const char *prog, const char *usage, FILE *s, int code) {
+static void usage_exit(const char *prog, const char *usage, int flags, FILE *s, int code) {
   fprintf(s, "Usage: %s %s\n", prog, usage);
-  fprintf(s,
-          "   -h --help                 Display this usage information.\n"
-          "   -p --parameters filename  Read the grid parameters from file.\n"
-          "   -i --input filename       Read input data from file.\n"
-          "   -o --output filename      Write output data to the file.\n"
-          "   -n --nthreads number      Number of host threads (text formatting).\n"
-          "      --device N             CUDA device ordinal (default 0).\n"
-          "      --binary               Also write OUTPUT.bin (raw FP64 results).\n");
+  fprintf(s, "   -h --help                 Display this usage information.\n"
+             "   -p --parameters filename  Read the grid parameters from file.\n");
+  if (!(flags & CLI_FUNCTION))
+    fprintf(s, "   -i --input filename       Read input data from file.\n");
+  fprintf(s, "   -o --output filename      Write output data to the file.\n"
+             "   -n --nthreads number      Number of host threads (text formatting).\n");
+  if (flags & CLI_FUNCTION)
+    fprintf(s, "      --function name        The test function: exponential_bump or\n"
+               "                             sinusoidal_bump (the reference's examples).\n");
+  fprintf(s, "      --device N             CUDA device ordinal (default 0).\n"
+             "      --binary               Also write OUTPUT.bin (raw FP64 results).\n");
   exit(code);
 }
 
 void cli_parse(int argc, char **argv, cli_args *a, const char *usage, int allow_small,
                int allow_sampler) {
+  cli_parse_flags(argc, argv, a, usage,
+                  (allow_small ? CLI_SMALL : 0) | (allow_sampler ? CLI_SAMPLER : 0));
+}
+
+void cli_parse_flags(int argc, char **argv, cli_args *a, const char *usage, int flags) {
+  const int allow_small = flags & CLI_SMALL, allow_sampler = flags & CLI_SAMPLER;
+  const int allow_function = flags & CLI_FUNCTION;
   memset(a, 0, sizeof(*a));
   a->nthreads = 1;
   a->sampler = WRT_SAMPLER_NEAREST;
+  a->function = -1;
   if (argc == 1) {
     fprintf(stderr, "%s: arguments required. Try '-h' or '--help'.\n", argv[0]);
     exit(EXIT_FAILURE);
   }
-  enum { OPT_DEVICE = 1000, OPT_BINARY, OPT_SAMPLER, OPT_HALF };
+  enum { OPT_DEVICE = 1000, OPT_BINARY, OPT_SAMPLER, OPT_HALF, OPT_FUNCTION };
   const struct option longopts[] = {
       {"help", no_argument, 0, 'h'},          {"parameters", required_argument, 0, 'p'},
       {"input", required_argument, 0, 'i'},   {"output", required_argument, 0, 'o'},
       {"nthreads", required_argument, 0, 'n'}, {"small", no_argument, 0, 's'},
       {"device", required_argument, 0, OPT_DEVICE}, {"binary", no_argument, 0, OPT_BINARY},
       {"sampler", required_argument, 0, OPT_SAMPLER},
-      {"half-extent", required_argument, 0, OPT_HALF}, {0, 0, 0, 0}};
-  const char *shortopts = allow_small ? "hp:i:so:n:" : "hp:i:o:n:";
+      {"half-extent", required_argument, 0, OPT_HALF},
+      {"function", required_argument, 0, OPT_FUNCTION}, {0, 0, 0, 0}};
+  /* the analytic programs take no input file (radon_analytic.c:131) */
+  const char *shortopts = allow_function ? "hp:o:n:" : allow_small ? "hp:i:so:n:" : "hp:i:o:n:";
   int c;
   while ((c = getopt_long(argc, argv, shortopts, longopts, NULL)) != -1) {
     switch (c) {
-      case 'h': usage_exit(argv[0], usage, stdout, 0); break;
+      case 'h': usage_exit(argv[0], usage, flags, stdout, 0); break;
       case 'p': a->params = optarg; printf("Parameters file: %s\n", optarg); break;
-      case 'i': a->input = optarg; printf("Input file: %s\n", optarg); break;
+      case 'i':
+        if (allow_function) usage_exit(argv[0], usage, flags, stderr, 1);
+        a->input = optarg;
+        printf("Input file: %s\n", optarg);
+        break;
       case 'o': a->output = optarg; printf("Output file: %s\n", optarg); break;
       case 'n':
         a->nthreads = atoi(optarg);
@@ -64,46 +81,69 @@ void cli_parse(int argc, char **argv, cli_args *a, const char *usage, int allow_
         printf("Number of threads: %d\n", a->nthreads);
         break;
       case 's':
-        if (!allow_small) usage_exit(argv[0], usage, stderr, 1);
+        if (!allow_small) usage_exit(argv[0], usage, flags, stderr, 1);
         a->small_format = 1;
         printf("Reading of the input in small format\n");
         break;
       case OPT_DEVICE: a->device = atoi(optarg); break;
       case OPT_BINARY: a->binary = 1; break;
       case OPT_SAMPLER:
-        if (!allow_sampler) usage_exit(argv[0], usage, stderr, 1);
+        if (!allow_sampler) usage_exit(argv[0], usage, flags, stderr, 1);
         if (!strcmp(optarg, "nearest")) a->sampler = WRT_SAMPLER_NEAREST;
         else if (!strcmp(optarg, "trilinear")) a->sampler = WRT_SAMPLER_TRILINEAR;
-        else usage_exit(argv[0], usage, stderr, 1);
+        else usage_exit(argv[0], usage, flags, stderr, 1);
         break;
       case OPT_HALF:
-        if (!allow_sampler) usage_exit(argv[0], usage, stderr, 1);
+        if (!allow_sampler) usage_exit(argv[0], usage, flags, stderr, 1);
         a->half_extent = atoi(optarg);
         break;
-      default: usage_exit(argv[0], usage, stderr, 1);
+      case OPT_FUNCTION:
+        if (!allow_function) usage_exit(argv[0], usage, flags, stderr, 1);
+        if (!strcmp(optarg, "exponential_bump")) a->function = WRT_FUNCTION_EXP_BUMP;
+        else if (!strcmp(optarg, "sinusoidal_bump")) a->function = WRT_FUNCTION_SINE_BUMPS;
+        else {
+          fprintf(stderr, "%s: unknown test function '%s' (exponential_bump or sinusoidal_bump)\n",
+                  argv[0], optarg);
+          exit(EXIT_FAILURE);
+        }
+        printf("Test function: %s\n", optarg);
+        break;
+      default: usage_exit(argv[0], usage, flags, stderr, 1);
     }
   }
   if (optind < argc) printf("Warning: non-option ARGV-arguments are omitted. See '-h' or '--help'.\n");
-  if (!a->params || !a->input || !a->output) {
+  if (allow_function) {
+    if (!a->params || !a->output) {
+      fprintf(stderr, "%s: -p and -o are required. Try '-h' or '--help'.\n", argv[0]);
+      exit(EXIT_FAILURE);
+    }
+    if (a->function < 0) {
+      fprintf(stderr, "%s: --function is required: exponential_bump or sinusoidal_bump (the "
+                      "reference compiles its test function in). Try '-h' or '--help'.\n", argv[0]);
+      exit(EXIT_FAILURE);
+    }
+  } else if (!a->params || !a->input || !a->output) {
     fprintf(stderr, "%s: -p, -i and -o are required. Try '-h' or '--help'.\n", argv[0]);
     exit(EXIT_FAILURE);
   }
 }
 
-int cli_read_params(const char *path, int p[4]) {
+int cli_read_params(const char *path, int p[4]) { return cli_read_params_n(path, p, 4); }
+
+int cli_read_params_n(const char *path, int *p, int count) {
   FILE *f = fopen(path, "r");
   if (!f) {
     fprintf(stderr, "Recieved call %s while opening %s. \n", strerror(errno), path);
     return -1;
   }
   char buffer[4096];
-  for (int k = 0; k < 4; ++k) {
-    int count = fscanf(f, "%d %4095[^\n]\n", &p[k], buffer);
-    if (count == EOF) {
+  for (int k = 0; k < count; ++k) {
+    const int got = fscanf(f, "%d %4095[^\n]\n", &p[k], buffer);
+    if (got == EOF) {
       fprintf(stderr, "Error: fscanf parameters %d : reached end of file before it was expected.\n", k);
       fclose(f);
       return -1;
-    } else if (count != 2) {
+    } else if (got != 2) {
       fprintf(stderr, "Error: fscanf parameters %d : matching failure, fscanf expected 1 integer value.\n", k);
       fclose(f);
       return -1;
@@ -372,6 +412,24 @@ void cli_readme(const char *output, const char *fmt, ...) {
   vfprintf(f, fmt, ap);
   va_end(ap);
   fclose(f);
+}
+
+void cli_example_function(int kind, wrt_function *f) {
+  memset(f, 0, sizeof(*f));
+  f->kind = kind;
+  if (kind == WRT_FUNCTION_EXP_BUMP) {
+    /* examples-test-functions/exponential_bump.c: centre (0.2, 0, 0), 0.5, eps 1e-2 */
+    const double p[5] = {0.2, 0.0, 0.0, 0.5, 1e-2};
+    f->count = 1;
+    memcpy(f->p, p, sizeof(p));
+  } else {
+    /* examples-test-functions/sinusoidal_bump.c: three balls
+     * (centre, amplitude, rin, rout) */
+    const double p[18] = {0.0, 0.2, 0.0, 1.0, 0.4, 0.6,  -0.5, 0.0, 0.0, 0.6, 0.3, 0.45,
+                          0.0, 0.2, 0.5, 0.3, 0.4, 0.6};
+    f->count = 3;
+    memcpy(f->p, p, sizeof(p));
+  }
 }
 
 wrt_ctx *cli_context(const cli_args *a) {

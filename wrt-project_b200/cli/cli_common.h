@@ -1,4 +1,4 @@
-/* cli_common.h -- shared pieces of the four drop-in programs.
+/* cli_common.h -- shared pieces of the drop-in programs.
  *
  * The programs keep the reference's command-line and file contract:
  *   -p FILE   parameter file: four lines "%d <text>" (each line must carry
@@ -26,13 +26,21 @@ typedef struct {
   int half_extent;  /* radon_grid --half-extent */
   int device;
   int binary;       /* also write OUT.bin: raw little-endian FP64 results */
+  int function;     /* radon_analytic / ray_analytic --function: a wrt_function_kind, -1 unset */
 } cli_args;
 
 /* usage: program-specific usage text; allow_small enables -s/--small. */
 void cli_parse(int argc, char **argv, cli_args *a, const char *usage, int allow_small,
                int allow_sampler);
+/* The same with option flags: CLI_SMALL (-s/--small), CLI_SAMPLER (--sampler,
+ * --half-extent), CLI_FUNCTION (the analytic programs: no -i, --function
+ * required). */
+enum { CLI_SMALL = 1, CLI_SAMPLER = 2, CLI_FUNCTION = 4 };
+void cli_parse_flags(int argc, char **argv, cli_args *a, const char *usage, int flags);
 /* Four integers from a parameter file; returns 0 or -1 (message printed). */
 int cli_read_params(const char *path, int p[4]);
+/* `count` integers, one per line "%d <text>" (ray_analytic reads three). */
+int cli_read_params_n(const char *path, int *p, int count);
 /* count doubles, one per line ("%lf\n"), parsed by nthreads threads; 0 or -1. */
 int cli_read_column(const char *path, size_t count, double *out, int nthreads);
 /* count lines "%lf, %lf, %lf, %lf"; keeps the 4th column; 0 or -1. */
@@ -44,6 +52,9 @@ int cli_write_rows(const char *path, size_t count, cli_row_fn row, const void *c
 int cli_write_binary(const char *path, const double *v, size_t count);
 /* "readme_<output>" with the given text (printf-style). */
 void cli_readme(const char *output, const char *fmt, ...);
+/* The reference's example test function of this kind (WRT_FUNCTION_*) with
+ * the constants of its example file. */
+void cli_example_function(int kind, wrt_function *f);
 wrt_ctx *cli_context(const cli_args *a);
 void cli_die_status(wrt_ctx *ctx, int st, const char *what);
 double cli_now(void);
