@@ -41,7 +41,10 @@ N, ELLIPSOIDS, SEED = 128, 16, 1001
 NPHI, NTHETA, NSHIFT = 128, 64, 256
 HALF_EXTENT = N  # lattice [-n, n)^2 -> 256 x 256 samples per plane
 BYTES_PER_SAMPLE = 32  # eight FP32 voxel reads per trilinear sample
-METRIC = "plane integrals/s @128^3 (64x128 sphere grid x 256 shifts, trilinear, 256^2 lattice)"
+# the headline metric's name as the benchmark's specification states it; the
+# workload itself (sphere grid, shifts, sampler, lattice) is spelled out in
+# each line's "config"
+METRIC = "plane integrals/s @128³ (served vs plain, same B200, rel.err≤1e-5); p50/p99 ms"
 UNIT = "plane integrals/s"
 
 
